@@ -1,0 +1,112 @@
+"""Pins the oracle: the NumPy and C restatements against golden vectors recorded
+from the unmodified reference source (tests/golden/make_golden.py)."""
+import numpy as np
+import pytest
+
+from oracle import c_oracle, fd_oracle
+from tests.conftest import load_golden, rel_l2, same_with_nan
+
+FWBW = ["fwbw_basic", "fwbw_topo", "fwbw_narrow", "fwbw_edge_source"]
+
+
+def _args(g):
+    return dict(dx=float(g["dx"]), dz=float(g["dz"]), nt=int(g["nt"]), fs=float(g["fs"]),
+                fw=int(g["fw"]))
+
+
+def _surface(g):
+    return g["surface"] if g["surface"].size else None
+
+
+@pytest.mark.parametrize("name", FWBW)
+def test_numpy_oracle_bit_exact_vs_reference(name):
+    """FP64 NumPy restatement == reference source run in FP64, bit for bit."""
+    g = load_golden(name)
+    sm, a = _surface(g), _args(g)
+    assert np.array_equal(fd_oracle.sponge(int(g["nx"]), int(g["nz"]), int(g["fw"])), g["absorb"])
+    m = fd_oracle.derived_material(g["mu_s"], g["lam_s"], g["rho_s"])
+    for k in ("mxz", "myx", "myz", "inv_rho", "inv_rho_u", "inv_rho_w"):
+        assert np.array_equal(m[k], g[k]), k
+    kw = dict(src=g["src"], wu=g["wu"], wv=g["wv"], ww=g["ww"], rec=g["rec"],
+              isnap=int(g["isnap"]), surface=sm, check_interval=0, **a)
+    obs = fd_oracle.forward(g["mu_t"], g["lam_t"], g["rho_t"], **kw)
+    syn = fd_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], save=True, **kw)
+    img = fd_oracle.backward(g["mu_s"], g["lam_s"], g["rho_s"], rec=g["rec"], ou=g["obs"][0],
+                             ov=g["obs"][1], ow=g["obs"][2], snaps=syn["snaps"],
+                             isnaps=syn["isnaps"], num_snaps=syn["num_snaps"],
+                             isnap=int(g["isnap"]), surface=sm, check_interval=0, **a)
+    assert np.array_equal(obs["seis"], g["obs"], equal_nan=True)
+    assert np.array_equal(syn["seis"], g["syn"], equal_nan=True)
+    if name != "fwbw_edge_source":
+        assert np.array_equal(syn["snaps"], g["snaps"], equal_nan=True)
+        assert np.array_equal(syn["isnaps"], g["isnaps"])
+        assert np.array_equal(img["img"], g["img"], equal_nan=True)
+
+
+@pytest.mark.parametrize("name", FWBW)
+def test_c_oracle_f64_vs_reference(name):
+    g = load_golden(name)
+    sm, a = _surface(g), _args(g)
+    kw = dict(src=g["src"], wu=g["wu"], wv=g["wv"], ww=g["ww"], rec=g["rec"],
+              isnap=int(g["isnap"]), surface=sm, check_interval=0, dtype=np.float64, **a)
+    f = c_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], save=True, **kw)
+    assert same_with_nan(f["seis"], g["syn"], rtol=1e-12, atol=1e-12 * np.nanmax(np.abs(g["syn"][np.isfinite(g["syn"])])))
+    snaps_ref_layout = np.moveaxis(f["snaps"], 1, -1)
+    b = c_oracle.backward(g["mu_s"], g["lam_s"], g["rho_s"], rec=g["rec"], obs=g["obs"],
+                          snaps=f["snaps"], isnaps=f["isnaps"], num_snaps=f["num_snaps"],
+                          isnap=int(g["isnap"]), surface=sm, check_interval=0,
+                          dtype=np.float64, **a)
+    if name != "fwbw_edge_source":
+        assert same_with_nan(snaps_ref_layout, g["snaps"], atol=1e-12 * np.abs(g["snaps"]).max())
+        assert rel_l2(b["img"], g["img"]) < 1e-12
+
+
+def test_edge_source_failure_code():
+    """A source on an edge cell multiplies by inv_rho_u = 1/0 (fm:304-307): the
+    first finite check (it = 0) reports code 3 (w beats u, fm:471-472)."""
+    g = load_golden("fwbw_edge_source")
+    a = _args(g)
+    kw = dict(src=g["src"], wu=g["wu"], wv=g["wv"], ww=g["ww"], rec=g["rec"], isnap=2, **a)
+    assert fd_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], **kw)["flag"] == 3
+    assert c_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], dtype=np.float64, **kw)["flag"] == 3
+    assert c_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], dtype=np.float32, **kw)["flag"] == 3
+
+
+def test_reference_f32_harmonic_mean_overflows():
+    """The reference's f32 4-point harmonic mean (fm:271-276) multiplies four
+    moduli; for mu ~ 1e10 Pa (Vp 3500 m/s rock) the product overflows f32 and
+    the run goes non-finite at the first check.  The FP64 set-up avoids it."""
+    nx, nz, nt = 24, 20, 12
+    mu = np.full((nx, nz), 1.0e10, np.float32)
+    lam = np.full((nx, nz), 1.2e10, np.float32)
+    rho = np.full((nx, nz), 2400.0, np.float32)
+    w = np.zeros((1, nt), np.float32)
+    w[0, 1] = 1.0
+    kw = dict(dx=5.0, dz=5.0, nt=nt, fs=2000.0, fw=4, src=[[12, 5]], wu=w, wv=w, ww=w,
+              rec=[[12, 1]], check_interval=1, dtype=np.float32)
+    assert c_oracle.forward(mu, lam, rho, setup_f64=False, **kw)["flag"] != 0
+    assert c_oracle.forward(mu, lam, rho, setup_f64=True, **kw)["flag"] == 0
+    m32 = fd_oracle.derived_material(mu, lam, rho, np.float32)
+    assert np.isinf(m32["mxz"][1:-1, 1:-1]).all()
+
+
+def test_c_f32_close_to_f64():
+    g = load_golden("fwbw_basic")
+    a = _args(g)
+    kw = dict(src=g["src"], wu=g["wu"], wv=g["wv"], ww=g["ww"], rec=g["rec"], **a)
+    f64 = c_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], dtype=np.float64, **kw)
+    f32 = c_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], dtype=np.float32, **kw)
+    assert rel_l2(f32["seis"], f64["seis"]) < 1e-5
+
+
+def test_modes_split_exact():
+    """P-SV and SH never read each other's fields (fm:330-384): running one
+    mode alone gives the same numbers for its components."""
+    g = load_golden("fwbw_basic")
+    a = _args(g)
+    kw = dict(src=g["src"], wu=g["wu"], wv=g["wv"], ww=g["ww"], rec=g["rec"], dtype=np.float64, **a)
+    both = c_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], modes=3, **kw)["seis"]
+    psv = c_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], modes=1, **kw)["seis"]
+    sh = c_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], modes=2, **kw)["seis"]
+    assert np.array_equal(both[[0, 2]], psv[[0, 2]])
+    assert np.array_equal(both[1], sh[1])
