@@ -1,0 +1,145 @@
+/* rtm_b200.h -- C ABI of the B200-native elastic RTM hot path.
+ *
+ * One library (taichirtm_b200/lib/librtm_b200.so) replaces the Taichi kernels
+ * and host time loops of TaichiRTM's src/forward_modeling.py and
+ * src/backward_modeling.py.  The reference has no FFI: its boundary is the
+ * Python classes ForwardModeling / BackwardModeling (exported from
+ * src/__init__.py:24-38).  Each entry point below names the reference code it
+ * replaces; the Python package taichirtm_b200 binds them with ctypes and keeps
+ * the reference's class and function names.
+ *
+ * Conventions
+ *   - Grid index i = x (rows), j = z (contiguous), arrays (nx, nz) row-major,
+ *     exactly the reference's field layout.
+ *   - All array pointers are DEVICE pointers unless the comment says "host".
+ *   - Every call is asynchronous on the given stream unless it returns
+ *     results in host memory (those synchronise the stream).
+ *   - Return value: 0 = success, negative = RTM_E_* error.  Per-shot
+ *     propagation status uses the reference's codes: 0 ok, 1/2/3 forward
+ *     non-finite u/v/w, 4/5/6 backward (forward_modeling.py:455-488,
+ *     backward_modeling.py:417-450); the highest code wins.
+ *   - A plan is not thread-safe; use one plan per host thread.
+ */
+#ifndef RTM_B200_H
+#define RTM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *rtm_stream_t; /* = cudaStream_t */
+typedef struct rtm_plan rtm_plan;
+
+enum {
+    RTM_OK = 0,
+    RTM_E_ARG = -1,      /* invalid argument (sizes, indices, null pointers) */
+    RTM_E_CUDA = -2,     /* a CUDA runtime call failed (see rtm_last_error) */
+    RTM_E_STATE = -3,    /* call out of order (e.g. propagate before set_model) */
+    RTM_E_NOMEM = -4,    /* device allocation failed */
+    RTM_E_RANGE = -5     /* size above a fixed limit of the entry point */
+};
+
+enum { RTM_PSV = 1, RTM_SH = 2, RTM_BOTH = 3 };
+
+/* Global grid and time axis: the kwargs nx, nz, dx, dz, nt, fs,
+ * absorbing_frame of ForwardModeling.__init__ (forward_modeling.py:126-135). */
+typedef struct {
+    int nx, nz;
+    double dx, dz;
+    double fs;            /* dt = 1 / fs (forward_modeling.py:135) */
+    int nt;
+    int absorbing_frame;  /* sponge width FW (forward_modeling.py:133, 237-241) */
+    int modes;            /* RTM_PSV | RTM_SH; RTM_BOTH is what the reference runs */
+} rtm_grid;
+
+/* One shot on a window of the global model: rows [x0, x0 + nx) (all columns).
+ * Source and receiver positions are LOCAL grid indices (i, j) in host memory,
+ * the contents of src_loc_field / recv_loc_field (forward_modeling.py:142-143).
+ * A window equal to the whole grid (x0 = 0, nx = grid nx) is the reference's
+ * single-shot run. */
+typedef struct {
+    int x0, nx;
+    int nsrc;
+    const int32_t *src_ij;  /* host, nsrc x 2 */
+    int nrec;
+    const int32_t *rec_ij;  /* host, nrec x 2 */
+} rtm_shot;
+
+/* Kernel launch shape (autotuned by the Python layer; 0 = default). */
+typedef struct {
+    int vec;        /* columns per lane: 1, 2 or 4 */
+    int rows;       /* rows per warp task */
+    int warps;      /* warps per CTA */
+} rtm_tune;
+
+/* Create a plan for nshots shots on one grid: validates geometry, builds the
+ * per-row source/receiver tables and the work list, allocates the
+ * ping-pong wavefield state.  Replaces ForwardModeling/BackwardModeling
+ * _init_fields (forward_modeling.py:155-190, backward_modeling.py:153-193). */
+int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots,
+                    const rtm_tune *tune, rtm_plan **out);
+int rtm_plan_destroy(rtm_plan *plan);
+
+/* Floats per padded row of the internal layout (row i at (i+1)*pitch + 4). */
+int rtm_plan_pitch(const rtm_plan *plan);
+/* Floats of ONE snapshot component for all shots of the plan and nsnap
+ * snapshots (layout per shot: [nsnap][nx_shot][pitch], shots back to back). */
+size_t rtm_plan_snapshot_floats(const rtm_plan *plan, int nsnap);
+
+/* Material set-up: derived fields (harmonic shear averages, arithmetic
+ * density averages, inverses) of ForwardModeling._init_material_from_fields,
+ * _compute_shear_avg, _compute_rho_avg, _compute_inv_rho
+ * (forward_modeling.py:192-201, 243-307) and the sponge profile of
+ * _init_absorbing (forward_modeling.py:203-241).  mu, lam, rho: (nx, nz)
+ * float32.  surface: (nx, nz) 0/1 topography mask or NULL
+ * (surface_matrix_field, forward_modeling.py:149, 412-419).  The averages are
+ * evaluated in double and rounded once to float. */
+int rtm_plan_set_model(rtm_plan *plan, const float *mu, const float *lam, const float *rho,
+                       const float *surface, rtm_stream_t stream);
+
+/* Forward propagation of every shot: ForwardModeling.run
+ * (forward_modeling.py:504-575), fused per time step.
+ *   wavelets: (3, nsrc_total, nt) u, v, w source wavelets, shots' sources in
+ *             plan order (wavelet_{u,v,w}_field).
+ *   seis:     (3, nrec_total, nt) output seismograms (seismogram_{u,v,w}).
+ *   save != 0: snapshots every isnap steps (it % isnap == 0, it != 0) into
+ *             snap_u/v/w (rtm_plan_snapshot_floats(plan, nt / isnap) floats
+ *             each; NULL for a component the plan does not propagate);
+ *             isnaps_out (host, nt / isnap) receives the saved step numbers.
+ *   check_interval: finite check every that many steps (0 = never).
+ *   flags:    host, nshots status codes (0 / 1..3). */
+int rtm_forward(rtm_plan *plan, const float *wavelets, float *seis, int save, int isnap,
+                float *snap_u, float *snap_v, float *snap_w, int32_t *isnaps_out,
+                int check_interval, int32_t *flags, rtm_stream_t stream);
+
+/* Backward (time-reversed) propagation with the zero-lag cross-correlation
+ * imaging condition: BackwardModeling.run_calc (backward_modeling.py:498-579)
+ * with _add_observed_data_kernel and _correlate_with_snapshot fused into the
+ * step.
+ *   obs:      (3, nrec_total, nt) observed data (obsdata_{u,v,w}_field).
+ *   snap_*:   forward snapshots (layout of rtm_forward), isnaps (host,
+ *             num_snaps) their step numbers, isnap the interval.
+ *   image:    (3, nx, nz) float32 per-shot image of shot 0 when nshots == 1
+ *             (result_{u,v,w}); may be NULL.
+ *   stack:    (3, grid nx, nz) float64; every shot's image is ADDED at its
+ *             window (the cross-shot sum of imaging.stack_rtm_images,
+ *             imaging.py:81-93); may be NULL.
+ *   flags:    host, nshots status codes (0 / 4..6). */
+int rtm_backward(rtm_plan *plan, const float *obs, const float *snap_u, const float *snap_v,
+                 const float *snap_w, const int32_t *isnaps, int num_snaps, int isnap,
+                 float *image, double *stack, int check_interval, int32_t *flags,
+                 rtm_stream_t stream);
+
+/* Diagnostics: kernels launched by the last propagate call, and the last
+ * error message of this thread. */
+long long rtm_plan_launch_count(const rtm_plan *plan);
+const char *rtm_last_error(void);
+const char *rtm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RTM_B200_H */

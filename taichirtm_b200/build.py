@@ -1,0 +1,49 @@
+"""Build librtm_b200.so in-tree for sm_100a (nvcc cross-compiles without a GPU).
+
+    python -m taichirtm_b200.build
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "lib")
+LIB = os.path.join(LIBDIR, "librtm_b200.so")
+SOURCES = ["rtm_api.cu"]
+DEPS = ["step_kernels.cuh", "aux_kernels.cuh", "adjoint_kernels.cuh", "noalloc.cu"]
+# -fmad=false: no FMA contraction, so every cell's FP32 arithmetic follows the
+# reference's expression order exactly and results do not depend on the launch
+# shape the autotuner picks (the kernels are HBM-bound; FLOPs are free).
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+              "-fmad=false", "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v"]
+
+
+def _stale():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    files = [os.path.join(CSRC, f) for f in SOURCES + DEPS]
+    files.append(os.path.join(HERE, "..", "include", "rtm_b200.h"))
+    return any(os.path.exists(f) and os.path.getmtime(f) > t for f in files)
+
+
+def build(force=False, verbose=False):
+    if not force and not _stale():
+        return LIB
+    os.makedirs(LIBDIR, exist_ok=True)
+    nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+    srcs = [os.path.join(CSRC, f) for f in SOURCES if os.path.exists(os.path.join(CSRC, f))]
+    cmd = [nvcc, *NVCC_FLAGS, *srcs, "-o", LIB + ".tmp"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed building librtm_b200.so")
+    if verbose:
+        sys.stderr.write(r.stderr)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

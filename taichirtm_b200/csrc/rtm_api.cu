@@ -1,0 +1,511 @@
+// Host side of librtm_b200: plans, time loops and the extern "C" entry
+// points declared in include/rtm_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rtm_b200.h"
+#include "aux_kernels.cuh"
+#include "step_kernels.cuh"
+
+using namespace rtm;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                  \
+    do {                                                                                \
+        cudaError_t e_ = (expr);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(e_ == cudaErrorMemoryAllocation ? RTM_E_NOMEM : RTM_E_CUDA,     \
+                        "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                      \
+    } while (0)
+
+template <typename T>
+int dalloc(T **p, size_t n) {
+    *p = nullptr;
+    if (n == 0) return 0;
+    CUDA_TRY(cudaMalloc((void **)p, n * sizeof(T)));
+    return 0;
+}
+
+int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+}  // namespace
+
+struct rtm_plan {
+    rtm_grid g{};
+    int nshots = 0;
+    int vec = 4, rows = 32, warps = 4;
+    int pitch = 0;
+    int nstrips = 0;
+    std::vector<ShotDev> shots_h;
+    ShotDev *d_shots = nullptr;
+    int4 *d_work = nullptr;
+    int n_work = 0;
+    int *d_src_ptr = nullptr, *d_rec_ptr = nullptr;
+    int2 *d_src_ent = nullptr, *d_rec_ent = nullptr;
+    int nsrc_total = 0, nrec_total = 0;
+    long long rows_total = 0;  // sum of nx over shots
+    size_t state_floats = 0;   // per field, per buffer
+    float *d_state[2][NFIELD] = {};
+    float *d_mat[NMAT] = {};
+    float *d_surface = nullptr;
+    bool has_surface = false;
+    float *d_sponge = nullptr;
+    float *d_img[3] = {}, *d_imgc[3] = {};
+    float *d_seis_t = nullptr, *d_obs_t = nullptr;
+    int *d_flags = nullptr;
+    bool model_set = false;
+    long long launches = 0;
+};
+
+namespace {
+
+bool field_active(int modes, int f) {
+    if (f == F_U || f == F_W || f == F_SXX || f == F_SZZ || f == F_SXZ) return modes & RTM_PSV;
+    return modes & RTM_SH;
+}
+bool comp_active(int modes, int c) { return c == 1 ? (modes & RTM_SH) : (modes & RTM_PSV); }
+
+void plan_free(rtm_plan *p) {
+    auto F = [](void *q) { if (q) cudaFree(q); };
+    F(p->d_shots); F(p->d_work); F(p->d_src_ptr); F(p->d_rec_ptr); F(p->d_src_ent); F(p->d_rec_ent);
+    for (int b = 0; b < 2; ++b) for (int f = 0; f < NFIELD; ++f) F(p->d_state[b][f]);
+    for (int m = 0; m < NMAT; ++m) F(p->d_mat[m]);
+    F(p->d_surface); F(p->d_sponge);
+    for (int c = 0; c < 3; ++c) { F(p->d_img[c]); F(p->d_imgc[c]); }
+    F(p->d_seis_t); F(p->d_obs_t); F(p->d_flags);
+}
+
+template <int DIR, int MODE, int VEC>
+cudaError_t launch_step(const StepParams &sp, int warps, cudaStream_t s) {
+    const int threads = 32 * warps;
+    const int blocks = (sp.n_work + warps - 1) / warps;
+    step_kernel<DIR, MODE, VEC><<<blocks, threads, 0, s>>>(sp);
+    return cudaGetLastError();
+}
+
+template <int DIR, int MODE>
+cudaError_t launch_vec(const StepParams &sp, int vec, int warps, cudaStream_t s) {
+    switch (vec) {
+        case 1: return launch_step<DIR, MODE, 1>(sp, warps, s);
+        case 2: return launch_step<DIR, MODE, 2>(sp, warps, s);
+        default: return launch_step<DIR, MODE, 4>(sp, warps, s);
+    }
+}
+
+template <int DIR>
+cudaError_t launch_mode(const StepParams &sp, int modes, int vec, int warps, cudaStream_t s) {
+    switch (modes) {
+        case RTM_PSV: return launch_vec<DIR, RTM_PSV>(sp, vec, warps, s);
+        case RTM_SH: return launch_vec<DIR, RTM_SH>(sp, vec, warps, s);
+        default: return launch_vec<DIR, RTM_BOTH>(sp, vec, warps, s);
+    }
+}
+
+void fill_common(const rtm_plan *p, StepParams &sp) {
+    std::memset(&sp, 0, sizeof sp);
+    const double dt = 1.0 / p->g.fs;
+    sp.nz = p->g.nz;
+    sp.pitch = p->pitch;
+    sp.nt = p->g.nt;
+    sp.fw = p->g.absorbing_frame;
+    sp.dt = (float)dt;
+    sp.inv_dx = (float)(1.0 / p->g.dx);
+    sp.inv_dz = (float)(1.0 / p->g.dz);
+    sp.src_factor = (float)(dt * p->g.dx * p->g.dz);  // forward_modeling.py:430
+    sp.sponge = p->d_sponge;
+    sp.work = p->d_work;
+    sp.n_work = p->n_work;
+    sp.shots = p->d_shots;
+    for (int m = 0; m < NMAT; ++m) sp.mat[m] = p->d_mat[m];
+    sp.surface = p->has_surface ? p->d_surface : nullptr;
+    sp.src_ptr = p->d_src_ptr;
+    sp.src_ent = p->d_src_ent;
+    sp.rec_ptr = p->d_rec_ptr;
+    sp.rec_ent = p->d_rec_ent;
+    sp.nrec_total = p->nrec_total;
+    sp.flags = p->d_flags;
+    sp.snap_k = -1;
+}
+
+int zero_state(rtm_plan *p, cudaStream_t s) {
+    for (int b = 0; b < 2; ++b)
+        for (int f = 0; f < NFIELD; ++f)
+            if (p->d_state[b][f])
+                CUDA_TRY(cudaMemsetAsync(p->d_state[b][f], 0, p->state_floats * sizeof(float), s));
+    CUDA_TRY(cudaMemsetAsync(p->d_flags, 0, p->nshots * sizeof(int), s));
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *rtm_version(void) { return "rtm_b200 1.0 (sm_100a)"; }
+const char *rtm_last_error(void) { return g_err.c_str(); }
+
+int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, const rtm_tune *tune,
+                    rtm_plan **out) {
+    if (!grid || !shots || !out || nshots <= 0) return fail(RTM_E_ARG, "null argument or nshots <= 0");
+    *out = nullptr;
+    const rtm_grid g = *grid;
+    if (g.nx < 3 || g.nz < 3) return fail(RTM_E_ARG, "grid must be at least 3x3 (nx=%d nz=%d)", g.nx, g.nz);
+    if (g.nt <= 0) return fail(RTM_E_ARG, "nt must be positive");
+    if (!(g.fs > 0) || !(g.dx > 0) || !(g.dz > 0)) return fail(RTM_E_ARG, "fs, dx, dz must be positive");
+    if (g.modes < 1 || g.modes > 3) return fail(RTM_E_ARG, "modes must be RTM_PSV, RTM_SH or RTM_BOTH");
+    if (g.absorbing_frame < 0 || g.absorbing_frame > g.nz)
+        return fail(RTM_E_ARG, "absorbing_frame %d outside [0, nz]", g.absorbing_frame);
+    rtm_plan *p = new rtm_plan();
+    p->g = g;
+    p->nshots = nshots;
+    if (tune) {
+        if (tune->vec == 1 || tune->vec == 2 || tune->vec == 4) p->vec = tune->vec;
+        if (tune->rows > 0) p->rows = tune->rows;
+        if (tune->warps > 0 && tune->warps <= 8) p->warps = tune->warps;
+    }
+    const int W = 30 * p->vec;
+    p->nstrips = (g.nz + W - 1) / W;
+    // Lanes touch columns [-vec, nstrips*W + vec); with 4 padding columns on
+    // the left this fits in ceil(nz/120)*120 + 8 for every vec, so the pitch
+    // (and every caller-visible layout) does not depend on the launch shape.
+    p->pitch = round_up(((g.nz + 119) / 120) * 120 + 8 + COL_OFF, 32);
+
+    // shots, row tables, work list
+    std::vector<int> src_ptr, rec_ptr;
+    std::vector<int2> src_ent, rec_ent;
+    std::vector<int4> work;
+    long long state_rows = 0;
+    for (int s = 0; s < nshots; ++s) {
+        const rtm_shot &sh = shots[s];
+        if (sh.nx < 3 || sh.x0 < 0 || sh.x0 + sh.nx > g.nx) {
+            delete p;
+            return fail(RTM_E_ARG, "shot %d window [%d, %d) outside grid nx=%d", s, sh.x0, sh.x0 + sh.nx, g.nx);
+        }
+        if (g.absorbing_frame > sh.nx) {
+            delete p;
+            return fail(RTM_E_ARG, "absorbing_frame %d wider than shot %d window (%d rows)", g.absorbing_frame, s, sh.nx);
+        }
+        if ((sh.nsrc > 0 && !sh.src_ij) || (sh.nrec > 0 && !sh.rec_ij) || sh.nsrc < 0 || sh.nrec < 0) {
+            delete p;
+            return fail(RTM_E_ARG, "shot %d: bad source/receiver arrays", s);
+        }
+        ShotDev d{};
+        d.nx = sh.nx;
+        d.x0 = sh.x0;
+        d.state_off = state_rows * p->pitch;
+        d.row_off = p->rows_total;
+        d.src_row0 = (int)src_ptr.size();
+        d.rec_row0 = (int)rec_ptr.size();
+        // per-row CSR, stable in the given order (duplicates accumulate in order)
+        auto build = [&](int n, const int32_t *ij, int base, std::vector<int> &ptr,
+                         std::vector<int2> &ent, const char *what) -> int {
+            std::vector<std::vector<int2>> byrow(sh.nx);
+            for (int k = 0; k < n; ++k) {
+                const int i = ij[2 * k], j = ij[2 * k + 1];
+                if (i < 0 || i >= sh.nx || j < 0 || j >= g.nz)
+                    return fail(RTM_E_ARG, "shot %d: %s %d at (%d, %d) outside the %dx%d window", s, what, k, i, j, sh.nx, g.nz);
+                byrow[i].push_back(make_int2(j, base + k));
+            }
+            for (int i = 0; i < sh.nx; ++i) {
+                ptr.push_back((int)ent.size());
+                for (auto &e : byrow[i]) ent.push_back(e);
+            }
+            ptr.push_back((int)ent.size());
+            return 0;
+        };
+        if (build(sh.nsrc, sh.src_ij, p->nsrc_total, src_ptr, src_ent, "source") ||
+            build(sh.nrec, sh.rec_ij, p->nrec_total, rec_ptr, rec_ent, "receiver")) {
+            delete p;
+            return RTM_E_ARG;
+        }
+        p->nsrc_total += sh.nsrc;
+        p->nrec_total += sh.nrec;
+        p->shots_h.push_back(d);
+        state_rows += sh.nx + 2;
+        p->rows_total += sh.nx;
+        for (int ia = 0; ia < sh.nx; ia += p->rows)
+            for (int st = 0; st < p->nstrips; ++st)
+                work.push_back(make_int4(s, st, ia, std::min(ia + p->rows, sh.nx)));
+    }
+    // Order tasks by global row so that concurrently running shots that
+    // overlap read the same material rows while they are in L2.
+    std::stable_sort(work.begin(), work.end(), [&](const int4 &a, const int4 &b) {
+        const int ga = p->shots_h[a.x].x0 + a.z, gb = p->shots_h[b.x].x0 + b.z;
+        if (ga != gb) return ga < gb;
+        if (a.y != b.y) return a.y < b.y;
+        return a.x < b.x;
+    });
+    p->n_work = (int)work.size();
+    p->state_floats = (size_t)state_rows * p->pitch;
+    const size_t mat_floats = (size_t)(g.nx + 2) * p->pitch;
+    const size_t img_floats = (size_t)p->rows_total * p->pitch;
+    int rc = 0;
+    rc |= dalloc(&p->d_shots, p->shots_h.size());
+    rc |= dalloc(&p->d_work, work.size());
+    rc |= dalloc(&p->d_src_ptr, src_ptr.size());
+    rc |= dalloc(&p->d_rec_ptr, rec_ptr.size());
+    rc |= dalloc(&p->d_src_ent, std::max<size_t>(src_ent.size(), 1));
+    rc |= dalloc(&p->d_rec_ent, std::max<size_t>(rec_ent.size(), 1));
+    rc |= dalloc(&p->d_flags, nshots);
+    rc |= dalloc(&p->d_sponge, std::max(g.absorbing_frame, 1));
+    for (int b = 0; b < 2 && !rc; ++b)
+        for (int f = 0; f < NFIELD && !rc; ++f)
+            if (field_active(g.modes, f)) rc |= dalloc(&p->d_state[b][f], p->state_floats);
+    for (int m = 0; m < NMAT && !rc; ++m) {
+        const bool need = (m <= M_MXZ) ? (g.modes & RTM_PSV) : (g.modes & RTM_SH);
+        if (need) rc |= dalloc(&p->d_mat[m], mat_floats);
+    }
+    rc |= dalloc(&p->d_surface, mat_floats);
+    for (int c = 0; c < 3 && !rc; ++c)
+        if (comp_active(g.modes, c)) {
+            rc |= dalloc(&p->d_img[c], img_floats);
+            rc |= dalloc(&p->d_imgc[c], img_floats);
+        }
+    rc |= dalloc(&p->d_seis_t, std::max<size_t>((size_t)3 * g.nt * p->nrec_total, 1));
+    rc |= dalloc(&p->d_obs_t, std::max<size_t>((size_t)3 * g.nt * p->nrec_total, 1));
+    if (rc) {
+        plan_free(p);
+        delete p;
+        return rc < 0 ? rc : RTM_E_NOMEM;
+    }
+    // sponge profile g(d) = exp(-(a (FW - d))^2), a = 0.0053 (forward_modeling.py:218-240)
+    std::vector<float> prof(std::max(g.absorbing_frame, 1), 1.0f);
+    const double a = 0.0053;
+    for (int d = 0; d < g.absorbing_frame; ++d) {
+        const double diff = (double)(g.absorbing_frame - d);
+        prof[d] = (float)std::exp((-(a * a) * diff) * diff);
+    }
+    auto H2D = [](void *dst, const void *src, size_t bytes) {
+        return bytes ? cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
+    };
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = H2D(p->d_shots, p->shots_h.data(), p->shots_h.size() * sizeof(ShotDev));
+    if (e == cudaSuccess) e = H2D(p->d_work, work.data(), work.size() * sizeof(int4));
+    if (e == cudaSuccess) e = H2D(p->d_src_ptr, src_ptr.data(), src_ptr.size() * sizeof(int));
+    if (e == cudaSuccess) e = H2D(p->d_rec_ptr, rec_ptr.data(), rec_ptr.size() * sizeof(int));
+    if (e == cudaSuccess) e = H2D(p->d_src_ent, src_ent.data(), src_ent.size() * sizeof(int2));
+    if (e == cudaSuccess) e = H2D(p->d_rec_ent, rec_ent.data(), rec_ent.size() * sizeof(int2));
+    if (e == cudaSuccess) e = H2D(p->d_sponge, prof.data(), prof.size() * sizeof(float));
+    if (e != cudaSuccess) {
+        plan_free(p);
+        delete p;
+        return fail(RTM_E_CUDA, "plan upload failed: %s", cudaGetErrorString(e));
+    }
+    *out = p;
+    return RTM_OK;
+}
+
+int rtm_plan_destroy(rtm_plan *p) {
+    if (!p) return RTM_OK;
+    plan_free(p);
+    delete p;
+    return RTM_OK;
+}
+
+int rtm_plan_pitch(const rtm_plan *p) { return p ? p->pitch : 0; }
+
+size_t rtm_plan_snapshot_floats(const rtm_plan *p, int nsnap) {
+    if (!p || nsnap <= 0) return 0;
+    return (size_t)nsnap * (size_t)p->rows_total * (size_t)p->pitch;
+}
+
+long long rtm_plan_launch_count(const rtm_plan *p) { return p ? p->launches : 0; }
+
+int rtm_plan_set_model(rtm_plan *p, const float *mu, const float *lam, const float *rho,
+                       const float *surface, rtm_stream_t stream) {
+    if (!p || !mu || !lam || !rho) return fail(RTM_E_ARG, "null model pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t mat_floats = (size_t)(p->g.nx + 2) * p->pitch;
+    for (int m = 0; m < NMAT; ++m)
+        if (p->d_mat[m]) CUDA_TRY(cudaMemsetAsync(p->d_mat[m], 0, mat_floats * sizeof(float), s));
+    CUDA_TRY(cudaMemsetAsync(p->d_surface, 0, mat_floats * sizeof(float), s));
+    const long long n = (long long)p->g.nx * p->g.nz;
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    setup_material_kernel<<<blocks, 256, 0, s>>>(
+        mu, lam, rho, surface, p->g.nx, p->g.nz, p->pitch, p->d_mat[M_IRU], p->d_mat[M_IRW],
+        p->d_mat[M_LAM], p->d_mat[M_MU], p->d_mat[M_MXZ], p->d_mat[M_IR], p->d_mat[M_MYX],
+        p->d_mat[M_MYZ], surface ? p->d_surface : nullptr);
+    CUDA_TRY(cudaGetLastError());
+    p->has_surface = surface != nullptr;
+    p->model_set = true;
+    return RTM_OK;
+}
+
+static int transpose(const float *in, float *out, int planes, int rows, int cols, cudaStream_t s) {
+    if (rows == 0 || cols == 0) return 0;
+    dim3 grid((cols + 31) / 32, (rows + 31) / 32, planes);
+    transpose_kernel<<<grid, dim3(32, 8), 0, s>>>(in, out, rows, cols);
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int isnap, float *snap_u,
+                float *snap_v, float *snap_w, int32_t *isnaps_out, int check_interval,
+                int32_t *flags, rtm_stream_t stream) {
+    if (!p) return fail(RTM_E_ARG, "null plan");
+    if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
+    if (p->nsrc_total > 0 && !wavelets) return fail(RTM_E_ARG, "null wavelets");
+    if (check_interval < 0) return fail(RTM_E_ARG, "check_interval < 0");
+    const int nt = p->g.nt;
+    int nsnap = 0;
+    if (save) {
+        if (isnap <= 0) return fail(RTM_E_ARG, "isnap must be positive");
+        nsnap = nt / isnap;  // forward_modeling.py:531
+        float *sp[3] = {snap_u, snap_v, snap_w};
+        for (int c = 0; c < 3; ++c)
+            if (comp_active(p->g.modes, c) && nsnap > 0 && !sp[c])
+                return fail(RTM_E_ARG, "snapshot buffer %d is null", c);
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    if (int rc = zero_state(p, s)) return rc;
+    const size_t nseis = (size_t)3 * nt * p->nrec_total;
+    if (nseis) CUDA_TRY(cudaMemsetAsync(p->d_seis_t, 0, nseis * sizeof(float), s));
+    StepParams sp;
+    fill_common(p, sp);
+    sp.code_base = 1;
+    const size_t plane = (size_t)nt * p->nrec_total;
+    for (int c = 0; c < 3; ++c) {
+        sp.wav[c] = wavelets ? wavelets + (size_t)c * p->nsrc_total * nt : nullptr;
+        sp.seis[c] = p->d_seis_t + c * plane;
+    }
+    sp.snap[0] = snap_u;
+    sp.snap[1] = snap_v;
+    sp.snap[2] = snap_w;
+    sp.nsnap = nsnap;
+    p->launches = 0;
+    for (int it = 0; it < nt; ++it) {
+        for (int f = 0; f < NFIELD; ++f) {
+            sp.sin[f] = p->d_state[it & 1][f];
+            sp.sout[f] = p->d_state[(it + 1) & 1][f];
+        }
+        sp.it = it;
+        sp.check = check_interval > 0 && it % check_interval == 0;
+        sp.snap_k = (save && it % isnap == 0 && it != 0) ? it / isnap - 1 : -1;  // fm:569-570
+        if (sp.snap_k >= nsnap) sp.snap_k = -1;
+        CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec, p->warps, s)));
+        ++p->launches;
+    }
+    if (seis && p->nrec_total) {
+        if (int rc = transpose(p->d_seis_t, seis, 3, nt, p->nrec_total, s)) return rc;
+        ++p->launches;
+    }
+    if (isnaps_out)
+        for (int k = 0; k < nsnap; ++k) {
+            const int it = (k + 1) * isnap;
+            isnaps_out[k] = it <= nt - 1 ? it : 0;  // fm:572; slots never reached stay 0
+        }
+    if (flags) {
+        CUDA_TRY(cudaMemcpyAsync(flags, p->d_flags, p->nshots * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    return RTM_OK;
+}
+
+int rtm_backward(rtm_plan *p, const float *obs, const float *snap_u, const float *snap_v,
+                 const float *snap_w, const int32_t *isnaps, int num_snaps, int isnap, float *image,
+                 double *stack, int check_interval, int32_t *flags, rtm_stream_t stream) {
+    if (!p) return fail(RTM_E_ARG, "null plan");
+    if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
+    if (p->nrec_total > 0 && !obs) return fail(RTM_E_ARG, "null observed data");
+    if (check_interval < 0) return fail(RTM_E_ARG, "check_interval < 0");
+    if (isnap <= 0) return fail(RTM_E_ARG, "isnap must be positive");
+    if (num_snaps < 0 || (num_snaps > 0 && !isnaps)) return fail(RTM_E_ARG, "bad snapshot table");
+    if (image && p->nshots != 1) return fail(RTM_E_ARG, "image output needs a single-shot plan; use stack");
+    const float *sp3[3] = {snap_u, snap_v, snap_w};
+    for (int c = 0; c < 3; ++c)
+        if (comp_active(p->g.modes, c) && num_snaps > 0 && !sp3[c])
+            return fail(RTM_E_ARG, "snapshot buffer %d is null", c);
+    const int nt = p->g.nt;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (int rc = zero_state(p, s)) return rc;
+    const size_t img_floats = (size_t)p->rows_total * p->pitch;
+    for (int c = 0; c < 3; ++c)
+        if (p->d_img[c]) {
+            CUDA_TRY(cudaMemsetAsync(p->d_img[c], 0, img_floats * sizeof(float), s));
+            CUDA_TRY(cudaMemsetAsync(p->d_imgc[c], 0, img_floats * sizeof(float), s));
+        }
+    if (p->nrec_total) {
+        if (int rc = transpose(obs, p->d_obs_t, 3, p->nrec_total, nt, s)) return rc;
+    }
+    StepParams sp;
+    fill_common(p, sp);
+    sp.code_base = 4;
+    const size_t plane = (size_t)nt * p->nrec_total;
+    for (int c = 0; c < 3; ++c) {
+        sp.obs[c] = p->d_obs_t + c * plane;
+        sp.snap[c] = const_cast<float *>(sp3[c]);
+        sp.img[c] = p->d_img[c];
+        sp.imgc[c] = p->d_imgc[c];
+    }
+    sp.nsnap = num_snaps;
+    p->launches = 1;
+    for (int it = 0; it < nt; ++it) {
+        const int t = (nt - 1) - it;  // backward_modeling.py:549
+        for (int f = 0; f < NFIELD; ++f) {
+            sp.sin[f] = p->d_state[it & 1][f];
+            sp.sout[f] = p->d_state[(it + 1) & 1][f];
+        }
+        sp.it = t;
+        sp.check = check_interval > 0 && it % check_interval == 0;
+        sp.snap_k = -1;
+        if (t > 0 && t % isnap == 0) {  // backward_modeling.py:558-564
+            const int k = t / isnap - 1;
+            if (k >= 0 && k < num_snaps && isnaps[k] == t) sp.snap_k = k;
+        }
+        CUDA_TRY((launch_mode<1>(sp, p->g.modes, p->vec, p->warps, s)));
+        ++p->launches;
+    }
+    const int blocks = 148 * 8;
+    if (image) {
+        const size_t n = (size_t)p->g.nx * p->g.nz;
+        for (int c = 0; c < 3; ++c) {
+            float *dst = image + c * n;
+            if (p->d_img[c]) {
+                image_out_kernel<<<blocks, 256, 0, s>>>(p->d_img[c], p->d_imgc[c], dst, 0,
+                                                        p->shots_h[0].nx, p->g.nz, p->pitch);
+                CUDA_TRY(cudaGetLastError());
+                ++p->launches;
+            } else {
+                CUDA_TRY(cudaMemsetAsync(dst, 0, n * sizeof(float), s));
+            }
+        }
+    }
+    if (stack) {
+        const size_t n = (size_t)p->g.nx * p->g.nz;
+        for (int c = 0; c < 3; ++c)
+            if (p->d_img[c]) {
+                stack_kernel<<<blocks, 256, 0, s>>>(p->d_img[c], p->d_imgc[c], stack + c * n, p->d_shots,
+                                                    p->nshots, p->g.nx, p->g.nz, p->pitch);
+                CUDA_TRY(cudaGetLastError());
+                ++p->launches;
+            }
+    }
+    if (flags) {
+        CUDA_TRY(cudaMemcpyAsync(flags, p->d_flags, p->nshots * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    return RTM_OK;
+}
+
+}  // extern "C"

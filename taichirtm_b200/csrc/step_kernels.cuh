@@ -1,0 +1,506 @@
+// Fused time-step kernels of the elastic O(2,2) staggered-grid propagator.
+//
+// One launch advances every shot of a plan by one time step.  It fuses the
+// reference's per-step kernel sequence
+//   forward  (src/forward_modeling.py:539-572):
+//     _set_free_surface/_set_surface_boundary, _update_velocity,
+//     _add_source_kernel, _update_stress, _apply_absorbing,
+//     _record_seismogram_kernel, _check_finite, _save_snapshot_kernel
+//   backward (src/backward_modeling.py:539-577):
+//     surface, _update_velocity_backward, _add_observed_data_kernel,
+//     _update_stress_backward, _apply_absorbing, _correlate_with_snapshot,
+//     _check_finite
+// into a single pass over the wavefield: state is read once from buffer A
+// and written once to buffer B (ping-pong), material is read once.
+//
+// Work decomposition.  Storage is (rows i = x) x (columns j = z, contiguous)
+// with a padded pitch; element (i, j) of a shot sits at
+// state_off + (i + 1) * pitch + (j + 4), so row -1 / row nx and columns
+// -4..-1 / nz.. are zero padding that halo reads may touch.  A warp owns a
+// strip of W = 30*VEC columns and a range of rows [ia, ib): lane L holds
+// columns c0 .. c0+VEC-1 with c0 = j0 - VEC + VEC*L, so lanes 1..30 own the
+// strip and lanes 0 / 31 carry the column halo.  The warp streams down the
+// rows; the stress row lags the velocity row by one, so every neighbour a
+// stencil needs is either in registers (previous row) or one warp shuffle
+// away (adjacent column).
+//
+// Semantics kept exactly (see the reference lines cited):
+//   * stencils update the interior only (1 <= i <= nx-2, 1 <= j <= nz-2);
+//     edge velocities change only by injection, edge stresses stay
+//     c * previous (they are zero);
+//   * sponge c(i, j) from the reference's loop order left -> right -> bottom
+//     (forward_modeling.py:211-235), evaluated from a 1-D profile;
+//   * the topography mask of the NEXT step's S0 multiplies sxz, szz, syz as
+//     they are written (nothing reads stress between S4 and the next S0);
+//   * sources add wavelet * (dt dx dz) * inv_rho at the source cell, with
+//     inv_rho_u / inv_rho_w = +inf on the shot's edge cells like the
+//     reference's 1 / 0 (forward_modeling.py:291-307, 421-443);
+//   * recorded, snapshotted, imaged and checked values are the velocities
+//     after absorbing (forward_modeling.py:550-572).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rtm {
+
+constexpr int COL_OFF = 4;
+constexpr unsigned FULL = 0xffffffffu;
+
+enum Field { F_U = 0, F_W, F_SXX, F_SZZ, F_SXZ, F_V, F_SYX, F_SYZ, NFIELD };
+enum Mat { M_IRU = 0, M_IRW, M_LAM, M_MU, M_MXZ, M_IR, M_MYX, M_MYZ, NMAT };
+
+struct ShotDev {
+    int nx, x0;          // rows of the window, first global row
+    long long state_off; // floats: the shot's padded block in each state field
+    long long row_off;   // sum of nx of earlier shots (compact per-shot blocks)
+    int src_row0;        // first entry of this shot's row table in src_ptr (nx+1 entries)
+    int rec_row0;        // same for rec_ptr
+};
+
+struct StepParams {
+    int nz, pitch, nt, fw;
+    float dt, inv_dx, inv_dz, src_factor;
+    const float *sponge;   // fw floats, profile by distance d = 0..fw-1
+    const int4 *work;      // (shot, strip, ia, ib) per warp task
+    int n_work;
+    const ShotDev *shots;
+    const float *sin[NFIELD];
+    float *sout[NFIELD];
+    const float *mat[NMAT];  // global model, padded like the state
+    const float *surface;    // global padded 0/1 mask, or nullptr
+    const int *src_ptr;
+    const int2 *src_ent;     // (j, source index)
+    const float *wav[3];     // (nsrc_total, nt) per component u, v, w
+    const int *rec_ptr;
+    const int2 *rec_ent;     // (j, receiver index)
+    int nrec_total;
+    float *seis[3];          // time-major (nt, nrec_total) per component
+    const float *obs[3];     // time-major (nt, nrec_total) per component
+    float *snap[3];          // per component: shots back to back, [nsnap][nx][pitch]
+    int nsnap, snap_k;       // snapshot slot written (forward) / read (backward); -1 none
+    float *img[3];           // per component Kahan sum, [row_off + i][pitch]
+    float *imgc[3];          // Kahan compensation
+    int check;               // run the finite check this step
+    int code_base;           // 1 forward, 4 backward
+    int *flags;              // per shot status
+    int it;                  // forward: step it; backward: reversed time t
+};
+
+template <int VEC>
+__device__ __forceinline__ void ldv(float (&v)[VEC], const float *__restrict__ p) {
+    if constexpr (VEC == 4) {
+        float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else if constexpr (VEC == 2) {
+        float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+        v[0] = t.x; v[1] = t.y;
+    } else {
+        v[0] = __ldg(p);
+    }
+}
+
+template <int VEC>
+__device__ __forceinline__ void stv(float *__restrict__ p, const float (&v)[VEC]) {
+    if constexpr (VEC == 4) {
+        *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else if constexpr (VEC == 2) {
+        *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]);
+    } else {
+        *p = v[0];
+    }
+}
+
+// forward_modeling.py:203-235: 1 everywhere, then left, right, bottom strips,
+// later strips overwriting earlier ones.
+__device__ __forceinline__ float sponge_coef(const StepParams &p, int nx, int i, int j) {
+    const int fw = p.fw, db = p.nz - 1 - j, dr = nx - 1 - i;
+    int d = -1;
+    if (i >= 0 && i < fw && db > i) d = i;
+    if (dr >= 0 && dr < fw && db > dr) d = dr;
+    if (db >= 0 && db < fw && i >= db && dr >= db) d = db;
+    return d >= 0 ? __ldg(p.sponge + d) : 1.0f;
+}
+
+__device__ __forceinline__ bool interior(int i, int j, int nx, int nz) {
+    return (unsigned)(i - 1) < (unsigned)(nx - 2) && (unsigned)(j - 1) < (unsigned)(nz - 2);
+}
+
+__device__ __forceinline__ int bad_code(float x, int code) {
+    return (isnan(x) || fabsf(x) > 1e30f) ? code : 0;
+}
+
+// Kahan update of one image cell: sum += prod with compensation comp.
+__device__ __forceinline__ void kahan_add(float &sum, float &comp, float prod) {
+    float y = __fsub_rn(prod, comp);
+    float t = __fadd_rn(sum, y);
+    comp = __fsub_rn(__fsub_rn(t, sum), y);
+    sum = t;
+}
+
+template <int DIR, int MODE, int VEC>
+__global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
+    constexpr bool PSV = (MODE & 1) != 0;
+    constexpr bool SH = (MODE & 2) != 0;
+    constexpr int W = 30 * VEC;
+    const int lane = threadIdx.x & 31;
+    const int task = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (task >= p.n_work) return;
+    const int4 wk = p.work[task];
+    if (__ldg(p.flags + wk.x) != 0) return;  // this shot already failed: stop it
+    const ShotDev sh = p.shots[wk.x];
+    const int nx = sh.nx, nz = p.nz, P = p.pitch;
+    const int j0 = wk.y * W;
+    const int c0 = j0 - VEC + VEC * lane;
+    const bool owner = lane >= 1 && lane <= 30;
+    const int ia = wk.z, ib = wk.w;
+    const long long soff = sh.state_off + (long long)(c0 + COL_OFF);
+    const long long moff = (long long)sh.x0 * P + (long long)(c0 + COL_OFF);
+    const float dt = p.dt, idx = p.inv_dx, idz = p.inv_dz;
+    const float sdt = DIR == 0 ? dt : -dt;
+    auto S = [&](int f, int i) { return p.sin[f] + soff + (long long)(i + 1) * P; };
+    auto M = [&](int m, int i) { return p.mat[m] + moff + (long long)(i + 1) * P; };
+
+    // stress of the previous and current row, velocities of the previous and
+    // current row (after the velocity update, before absorbing), sponge
+    float sxx_p[VEC], szz_p[VEC], sxz_p[VEC], syx_p[VEC], syz_p[VEC];
+    float sxx_c[VEC], szz_c[VEC], sxz_c[VEC], syx_c[VEC], syz_c[VEC];
+    float u_p[VEC], w_p[VEC], v_p[VEC], u_c[VEC], w_c[VEC], v_c[VEC];
+    float vs_u[VEC], vs_w[VEC], vs_v[VEC], ir_u[VEC], ir_w[VEC], ir_v[VEC];
+    float cc[VEC];
+    int code = 0;
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+        u_p[q] = w_p[q] = v_p[q] = 0.f;
+        u_c[q] = w_c[q] = v_c[q] = 0.f;
+    }
+
+    auto load_sigma = [&](int i, float (&xx)[VEC], float (&zz)[VEC], float (&xz)[VEC],
+                          float (&yx)[VEC], float (&yz)[VEC]) {
+        if constexpr (PSV) {
+            ldv<VEC>(xx, S(F_SXX, i));
+            ldv<VEC>(zz, S(F_SZZ, i));
+            ldv<VEC>(xz, S(F_SXZ, i));
+        }
+        if constexpr (SH) {
+            ldv<VEC>(yx, S(F_SYX, i));
+            ldv<VEC>(yz, S(F_SYZ, i));
+        }
+    };
+    auto load_vel = [&](int i) {
+        if constexpr (PSV) {
+            ldv<VEC>(vs_u, S(F_U, i));
+            ldv<VEC>(vs_w, S(F_W, i));
+            ldv<VEC>(ir_u, M(M_IRU, i));
+            ldv<VEC>(ir_w, M(M_IRW, i));
+        }
+        if constexpr (SH) {
+            ldv<VEC>(vs_v, S(F_V, i));
+            ldv<VEC>(ir_v, M(M_IR, i));
+        }
+    };
+    // Point injection into the velocities of row i (held in u_c/w_c/v_c):
+    // forward sources (forward_modeling.py:421-443) or backward observed data
+    // (backward_modeling.py:452-460).  Every lane that computes a column does
+    // it, halo lanes included, so halo velocities are exact.
+    auto inject = [&](int i) {
+        if (i < 0 || i >= nx) return;
+        if constexpr (DIR == 0) {
+            const int e0 = __ldg(p.src_ptr + sh.src_row0 + i), e1 = __ldg(p.src_ptr + sh.src_row0 + i + 1);
+            for (int e = e0; e < e1; ++e) {
+                const int2 en = __ldg(p.src_ent + e);
+                const int q = en.x - c0;
+                if (q < 0 || q >= VEC) continue;
+                const bool in = interior(i, en.x, nx, nz);
+                const float f = p.src_factor;
+                const size_t t = (size_t)en.y * p.nt + p.it;
+#pragma unroll
+                for (int qq = 0; qq < VEC; ++qq) {
+                    if (qq != q) continue;
+                    if constexpr (PSV) {
+                        u_c[qq] += __ldg(p.wav[0] + t) * f * (in ? ir_u[qq] : __int_as_float(0x7f800000));
+                        w_c[qq] += __ldg(p.wav[2] + t) * f * (in ? ir_w[qq] : __int_as_float(0x7f800000));
+                    }
+                    if constexpr (SH) v_c[qq] += __ldg(p.wav[1] + t) * f * ir_v[qq];
+                }
+            }
+        } else {
+            const int e0 = __ldg(p.rec_ptr + sh.rec_row0 + i), e1 = __ldg(p.rec_ptr + sh.rec_row0 + i + 1);
+            for (int e = e0; e < e1; ++e) {
+                const int2 en = __ldg(p.rec_ent + e);
+                const int q = en.x - c0;
+                if (q < 0 || q >= VEC) continue;
+                const size_t t = (size_t)p.it * p.nrec_total + en.y;
+#pragma unroll
+                for (int qq = 0; qq < VEC; ++qq) {
+                    if (qq != q) continue;
+                    if constexpr (PSV) {
+                        u_c[qq] += __ldg(p.obs[0] + t);
+                        w_c[qq] += __ldg(p.obs[2] + t);
+                    }
+                    if constexpr (SH) v_c[qq] += __ldg(p.obs[1] + t);
+                }
+            }
+        }
+    };
+    // Stress update of row r from the velocities of rows r and r+1 (forward)
+    // or r-1 and r (backward); writes stress and absorbed velocity of row r,
+    // then records / snapshots / images / checks it.
+    auto finish_row = [&](int r, const float (&cr)[VEC], const float (&va_u)[VEC],
+                          const float (&va_w)[VEC], const float (&va_v)[VEC],
+                          const float (&vb_u)[VEC], const float (&vb_w)[VEC],
+                          const float (&vb_v)[VEC]) {
+        // va = velocities of row r, vb = the other row (r+1 forward, r-1 backward)
+        float lam[VEC], mu[VEC], mxz[VEC], myx[VEC], myz[VEC], sm[VEC];
+        if constexpr (PSV) {
+            ldv<VEC>(lam, M(M_LAM, r));
+            ldv<VEC>(mu, M(M_MU, r));
+            ldv<VEC>(mxz, M(M_MXZ, r));
+        }
+        if constexpr (SH) {
+            ldv<VEC>(myx, M(M_MYX, r));
+            ldv<VEC>(myz, M(M_MYZ, r));
+        }
+        if (p.surface) {
+            ldv<VEC>(sm, p.surface + moff + (long long)(r + 1) * P);
+        } else {
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) sm[q] = 1.f;
+        }
+        // column neighbour of row r's velocities: j+1 (forward) or j-1 (backward)
+        float nu = 0.f, nw = 0.f, nv = 0.f;
+        if constexpr (DIR == 0) {
+            if constexpr (PSV) { nu = __shfl_down_sync(FULL, va_u[0], 1); nw = __shfl_down_sync(FULL, va_w[0], 1); }
+            if constexpr (SH) nv = __shfl_down_sync(FULL, va_v[0], 1);
+        } else {
+            if constexpr (PSV) { nu = __shfl_up_sync(FULL, va_u[VEC - 1], 1); nw = __shfl_up_sync(FULL, va_w[VEC - 1], 1); }
+            if constexpr (SH) nv = __shfl_up_sync(FULL, va_v[VEC - 1], 1);
+        }
+        float o_sxx[VEC], o_szz[VEC], o_sxz[VEC], o_syx[VEC], o_syz[VEC];
+        float o_u[VEC], o_w[VEC], o_v[VEC];
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            const int j = c0 + q;
+            const bool in = interior(r, j, nx, nz);
+            if constexpr (PSV) {
+                float u_x, u_z, w_x, w_z;
+                if constexpr (DIR == 0) {
+                    const float uj = q < VEC - 1 ? va_u[q + 1] : nu;
+                    const float wj = q < VEC - 1 ? va_w[q + 1] : nw;
+                    u_x = (vb_u[q] - va_u[q]) * idx;   // fm:369
+                    u_z = (uj - va_u[q]) * idz;        // fm:370
+                    w_x = (vb_w[q] - va_w[q]) * idx;   // fm:371
+                    w_z = (wj - va_w[q]) * idz;        // fm:372
+                } else {
+                    const float uj = q > 0 ? va_u[q - 1] : nu;
+                    const float wj = q > 0 ? va_w[q - 1] : nw;
+                    u_x = (va_u[q] - vb_u[q]) * idx;   // bm:366
+                    u_z = (va_u[q] - uj) * idz;        // bm:367
+                    w_x = (va_w[q] - vb_w[q]) * idx;   // bm:368
+                    w_z = (va_w[q] - wj) * idz;        // bm:369
+                }
+                const float div = u_x + w_z;
+                float sxx = sxx_p[q] + sdt * (lam[q] * div + 2.0f * mu[q] * u_x);
+                float szz = szz_p[q] + sdt * (lam[q] * div + 2.0f * mu[q] * w_z);
+                float sxz = sxz_p[q] + sdt * mxz[q] * (u_z + w_x);
+                sxx = in ? sxx : sxx_p[q];
+                szz = in ? szz : szz_p[q];
+                sxz = in ? sxz : sxz_p[q];
+                o_sxx[q] = cr[q] * sxx;
+                o_szz[q] = (cr[q] * szz) * sm[q];
+                o_sxz[q] = (cr[q] * sxz) * sm[q];
+                o_u[q] = cr[q] * va_u[q];
+                o_w[q] = cr[q] * va_w[q];
+            }
+            if constexpr (SH) {
+                float v_x, v_z;
+                if constexpr (DIR == 0) {
+                    const float vj = q < VEC - 1 ? va_v[q + 1] : nv;
+                    v_x = (vb_v[q] - va_v[q]) * idx;   // fm:381
+                    v_z = (vj - va_v[q]) * idz;        // fm:382
+                } else {
+                    const float vj = q > 0 ? va_v[q - 1] : nv;
+                    v_x = (va_v[q] - vb_v[q]) * idx;   // bm:377
+                    v_z = (va_v[q] - vj) * idz;        // bm:378
+                }
+                float syx = syx_p[q] + sdt * myx[q] * v_x;
+                float syz = syz_p[q] + sdt * myz[q] * v_z;
+                syx = in ? syx : syx_p[q];
+                syz = in ? syz : syz_p[q];
+                o_syx[q] = cr[q] * syx;
+                o_syz[q] = (cr[q] * syz) * sm[q];
+                o_v[q] = cr[q] * va_v[q];
+            }
+        }
+        if (!owner) return;
+        const long long so = soff + (long long)(r + 1) * P;
+        if constexpr (PSV) {
+            stv<VEC>(p.sout[F_SXX] + so, o_sxx);
+            stv<VEC>(p.sout[F_SZZ] + so, o_szz);
+            stv<VEC>(p.sout[F_SXZ] + so, o_sxz);
+            stv<VEC>(p.sout[F_U] + so, o_u);
+            stv<VEC>(p.sout[F_W] + so, o_w);
+        }
+        if constexpr (SH) {
+            stv<VEC>(p.sout[F_SYX] + so, o_syx);
+            stv<VEC>(p.sout[F_SYZ] + so, o_syz);
+            stv<VEC>(p.sout[F_V] + so, o_v);
+        }
+        if constexpr (DIR == 0) {
+            // _record_seismogram_kernel (forward_modeling.py:445-453)
+            const int e0 = __ldg(p.rec_ptr + sh.rec_row0 + r), e1 = __ldg(p.rec_ptr + sh.rec_row0 + r + 1);
+            for (int e = e0; e < e1; ++e) {
+                const int2 en = __ldg(p.rec_ent + e);
+                const int q = en.x - c0;
+                if (q < 0 || q >= VEC) continue;
+                const size_t t = (size_t)p.it * p.nrec_total + en.y;
+#pragma unroll
+                for (int qq = 0; qq < VEC; ++qq) {
+                    if (qq != q) continue;
+                    if constexpr (PSV) { p.seis[0][t] = o_u[qq]; p.seis[2][t] = o_w[qq]; }
+                    if constexpr (SH) p.seis[1][t] = o_v[qq];
+                }
+            }
+            // _save_snapshot_kernel (forward_modeling.py:490-497, 569-572)
+            if (p.snap_k >= 0) {
+                const long long o = ((long long)p.nsnap * sh.row_off + (long long)p.snap_k * nx + r) * P + c0 + COL_OFF;
+                if constexpr (PSV) { stv<VEC>(p.snap[0] + o, o_u); stv<VEC>(p.snap[2] + o, o_w); }
+                if constexpr (SH) stv<VEC>(p.snap[1] + o, o_v);
+            }
+        } else {
+            // _correlate_with_snapshot (backward_modeling.py:481-488), Kahan-compensated
+            if (p.snap_k >= 0) {
+                const long long o = ((long long)p.nsnap * sh.row_off + (long long)p.snap_k * nx + r) * P + c0 + COL_OFF;
+                const long long io = (sh.row_off + r) * (long long)P + c0 + COL_OFF;
+                auto image = [&](int c, const float (&ov)[VEC]) {
+                    float s[VEC], sum[VEC], cmp[VEC];
+                    ldv<VEC>(s, p.snap[c] + o);
+                    ldv<VEC>(sum, p.img[c] + io);
+                    ldv<VEC>(cmp, p.imgc[c] + io);
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) kahan_add(sum[q], cmp[q], __fmul_rn(s[q], ov[q]));
+                    stv<VEC>(p.img[c] + io, sum);
+                    stv<VEC>(p.imgc[c] + io, cmp);
+                };
+                if constexpr (PSV) { image(0, o_u); image(2, o_w); }
+                if constexpr (SH) image(1, o_v);
+            }
+        }
+        // _check_finite (forward_modeling.py:455-488, backward_modeling.py:417-450)
+        if (p.check) {
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                if constexpr (PSV) {
+                    code = max(code, bad_code(o_u[q], p.code_base));
+                    code = max(code, bad_code(o_w[q], p.code_base + 2));
+                }
+                if constexpr (SH) code = max(code, bad_code(o_v[q], p.code_base + 1));
+            }
+        }
+    };
+
+    if constexpr (DIR == 0) {
+        // ---------------- forward: velocity row k, stress row k-1 ----------------
+        load_sigma(ia - 1, sxx_p, szz_p, sxz_p, syx_p, syz_p);
+        float c_prev[VEC];
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) c_prev[q] = 1.f;
+        for (int k = ia; k <= ib; ++k) {
+            load_sigma(k, sxx_c, szz_c, sxz_c, syx_c, syz_c);
+            load_vel(k);
+            float szz_m = 0.f, sxz_m = 0.f, syz_m = 0.f;  // column j-1 of row k
+            if constexpr (PSV) {
+                szz_m = __shfl_up_sync(FULL, szz_c[VEC - 1], 1);
+                sxz_m = __shfl_up_sync(FULL, sxz_c[VEC - 1], 1);
+            }
+            if constexpr (SH) syz_m = __shfl_up_sync(FULL, syz_c[VEC - 1], 1);
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                const int j = c0 + q;
+                const bool in = interior(k, j, nx, nz);
+                cc[q] = sponge_coef(p, nx, k, j);
+                if constexpr (PSV) {
+                    const float sxz_jm = q > 0 ? sxz_c[q - 1] : sxz_m;
+                    const float szz_jm = q > 0 ? szz_c[q - 1] : szz_m;
+                    const float sxx_x = (sxx_c[q] - sxx_p[q]) * idx;  // fm:332
+                    const float szz_z = (szz_c[q] - szz_jm) * idz;    // fm:333
+                    const float sxz_x = (sxz_c[q] - sxz_p[q]) * idx;  // fm:334
+                    const float sxz_z = (sxz_c[q] - sxz_jm) * idz;    // fm:335
+                    const float du = (sxx_x + sxz_z) * dt * ir_u[q];  // fm:339
+                    const float dw = (sxz_x + szz_z) * dt * ir_w[q];  // fm:340
+                    u_c[q] = in ? vs_u[q] + du : vs_u[q];
+                    w_c[q] = in ? vs_w[q] + dw : vs_w[q];
+                }
+                if constexpr (SH) {
+                    const float syz_jm = q > 0 ? syz_c[q - 1] : syz_m;
+                    const float syx_x = (syx_c[q] - syx_p[q]) * idx;  // fm:343
+                    const float syz_z = (syz_c[q] - syz_jm) * idz;    // fm:344
+                    const float dv = (syx_x + syz_z) * dt * ir_v[q];  // fm:347
+                    v_c[q] = in ? vs_v[q] + dv : vs_v[q];
+                }
+            }
+            inject(k);
+            if (k > ia) finish_row(k - 1, c_prev, u_p, w_p, v_p, u_c, w_c, v_c);
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                sxx_p[q] = sxx_c[q]; szz_p[q] = szz_c[q]; sxz_p[q] = sxz_c[q];
+                syx_p[q] = syx_c[q]; syz_p[q] = syz_c[q];
+                u_p[q] = u_c[q]; w_p[q] = w_c[q]; v_p[q] = v_c[q];
+                c_prev[q] = cc[q];
+            }
+        }
+    } else {
+        // ------------- backward: velocity row k-1 (needs stress row k) -------------
+        load_sigma(ia - 1, sxx_p, szz_p, sxz_p, syx_p, syz_p);
+        load_vel(ia - 1);
+        for (int k = ia; k <= ib; ++k) {
+            const int r = k - 1;
+            load_sigma(k, sxx_c, szz_c, sxz_c, syx_c, syz_c);
+            float szz_n = 0.f, sxz_n = 0.f, syz_n = 0.f;  // column j+1 of row r
+            if constexpr (PSV) {
+                szz_n = __shfl_down_sync(FULL, szz_p[0], 1);
+                sxz_n = __shfl_down_sync(FULL, sxz_p[0], 1);
+            }
+            if constexpr (SH) syz_n = __shfl_down_sync(FULL, syz_p[0], 1);
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                const int j = c0 + q;
+                const bool in = interior(r, j, nx, nz);
+                cc[q] = sponge_coef(p, nx, r, j);
+                if constexpr (PSV) {
+                    const float sxz_jp = q < VEC - 1 ? sxz_p[q + 1] : sxz_n;
+                    const float szz_jp = q < VEC - 1 ? szz_p[q + 1] : szz_n;
+                    const float sxx_x = (sxx_c[q] - sxx_p[q]) * idx;  // bm:333
+                    const float szz_z = (szz_jp - szz_p[q]) * idz;    // bm:334
+                    const float sxz_x = (sxz_c[q] - sxz_p[q]) * idx;  // bm:335
+                    const float sxz_z = (sxz_jp - sxz_p[q]) * idz;    // bm:336
+                    const float du = -(sxx_x + sxz_z) * dt * ir_u[q]; // bm:340
+                    const float dw = -(sxz_x + szz_z) * dt * ir_w[q]; // bm:341
+                    u_c[q] = in ? vs_u[q] + du : vs_u[q];
+                    w_c[q] = in ? vs_w[q] + dw : vs_w[q];
+                }
+                if constexpr (SH) {
+                    const float syz_jp = q < VEC - 1 ? syz_p[q + 1] : syz_n;
+                    const float syx_x = (syx_c[q] - syx_p[q]) * idx;  // bm:343
+                    const float syz_z = (syz_jp - syz_p[q]) * idz;    // bm:344
+                    const float dv = -(syx_x + syz_z) * dt * ir_v[q]; // bm:345
+                    v_c[q] = in ? vs_v[q] + dv : vs_v[q];
+                }
+            }
+            inject(r);
+            if (k > ia) finish_row(r, cc, u_c, w_c, v_c, u_p, w_p, v_p);
+            if (k < ib) load_vel(k);
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                sxx_p[q] = sxx_c[q]; szz_p[q] = szz_c[q]; sxz_p[q] = sxz_c[q];
+                syx_p[q] = syx_c[q]; syz_p[q] = syz_c[q];
+                u_p[q] = u_c[q]; w_p[q] = w_c[q]; v_p[q] = v_c[q];
+            }
+        }
+    }
+    if (p.check) {
+        code = __reduce_max_sync(FULL, code);
+        if (lane == 0 && code > 0) atomicMax(p.flags + wk.x, code);
+    }
+}
+
+}  // namespace rtm
