@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark: batched P-SV reverse-time migration on one B200 (per GPU).
+
+Workload (one "step"): 64 shots of the batched P-SV RTM configuration -- a
+2001 x 801 model (dx = 5 m, dt = 0.5 ms, nt = 3000, 4 layers + 20 seeded
+anomalies), shot k at x index 55 + 30 k with U{200..800} receivers in a window
++- a 50-cell sponge -- migrated in one pass: forward with snapshots every 16
+steps, backward with Kahan zero-lag cross-correlation, FP64 stack of all 64
+images on the global grid.  Each time step of each phase is ONE kernel launch
+covering all 64 shots.  Observed data are modelled on the true model before
+timing.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun every rank migrates its own 64-shot batch (weak scaling) and
+the stacked images are summed across ranks with one FP64 all-reduce.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RTM shots/s & Gcell-upd/s, batched vs plain on one B200, at <=1e-4 image err"
+ISNAP = 16
+BYTES_PER_CELL = 60          # P-SV: 5 state fields read+written (40 B) + 5 material reads (20 B)
+SNAP_BYTES_PER_CELL = 8      # forward snapshot step: u, w written
+IMG_BYTES_PER_CELL = 40      # imaging step: u, w snapshot read (8) + Kahan sum/comp RMW (32)
+PEAK_FALLBACK_GBS = 6650.0
+
+
+def workload_desc(nshots, nt):
+    return (f"batched P-SV RTM: {nshots} shots on a 2001x801 model (dx=5 m, dt=0.5 ms, nt={nt}), "
+            "windows of U{200..800} receivers +- 50-cell sponge, isnap=16, Kahan imaging, FP64 stack")
+
+
+def peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return PEAK_FALLBACK_GBS, "fallback"
+
+
+def ncu_traffic_per_cell():
+    """DRAM bytes per cell-update of the step kernel from the committed ncu
+    summary (profiles/step_kernel_traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "step_kernel_traffic.json")) as f:
+            return float(json.load(f)["dram_bytes_per_cell_update"])
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self, gpu_index=None):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if gpu_index is not None:
+            sel = [r for r in rows if r[0].strip() == str(gpu_index)]
+            rows = sel or rows
+        if not rows:
+            return None
+        sm = np.array([float(r[1]) for r in rows])
+        mx = max(float(r[2]) for r in rows)
+        pw = np.array([float(r[3]) if r[3].strip() not in ("[N/A]", "N/A") else 0 for r in rows])
+        load = sm[pw > 0.5 * pw.max()] if pw.max() > 0 else sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return dict(sm_mhz=float(np.median(load)), sm_max_mhz=mx, reasons=reasons, samples=len(rows))
+
+
+def build_workload(nt):
+    from taichirtm_b200 import synthetic as S
+    return S.config3(nt=nt)
+
+
+# --------------------------------------------------------------------------- CPU
+def cpu_rtm_sample(survey, target_s=12.0, modes=3):
+    """The reference algorithm on the host cores (C/OpenMP FP32 restatement of
+    src/forward_modeling.py + src/backward_modeling.py, both P-SV and SH as the
+    reference always advances): one shot of the workload, the time loop
+    truncated to a bounded number of steps per phase, scaled to one shot."""
+    from oracle import c_oracle
+    sh = survey.shots[0]
+    mu, lam, rho = survey.material(migration=True)
+    mu, lam, rho = (np.ascontiguousarray(x[sh.x0:sh.x0 + sh.nx]) for x in (mu, lam, rho))
+    nthreads = os.cpu_count() or 1
+    nt = survey.nt
+    kw = dict(dx=survey.dx, dz=survey.dz, nt=nt, fs=survey.fs, fw=survey.fw, dtype=np.float32,
+              modes=modes, nthreads=nthreads)
+    probe = 20
+    t0 = time.perf_counter()
+    c_oracle.forward(mu, lam, rho, src=sh.src, wu=sh.wavelets[0], wv=sh.wavelets[1], ww=sh.wavelets[2],
+                     rec=sh.rec, nt_run=probe, **kw)
+    per_step = (time.perf_counter() - t0) / probe
+    n_run = int(max(20, min(nt, target_s / 2.0 / max(per_step, 1e-6))))
+    t0 = time.perf_counter()
+    f = c_oracle.forward(mu, lam, rho, src=sh.src, wu=sh.wavelets[0], wv=sh.wavelets[1], ww=sh.wavelets[2],
+                         rec=sh.rec, nt_run=n_run, save=True, isnap=ISNAP, **kw)
+    t_f = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    c_oracle.backward(mu, lam, rho, rec=sh.rec, obs=np.zeros((3, len(sh.rec), nt), np.float32),
+                      snaps=f["snaps"], isnaps=np.arange(1, nt // ISNAP + 1) * ISNAP,
+                      num_snaps=nt // ISNAP, isnap=ISNAP, nt_run=n_run, **kw)
+    t_b = time.perf_counter() - t0
+    sec_per_shot = (t_f + t_b) * nt / n_run
+    cells = sh.nx * survey.nz
+    return dict(value=1.0 / sec_per_shot, unit="shots/s", cores=nthreads, kind="port",
+                gcell_upd_per_s=2 * cells * nt / sec_per_shot / 1e9,
+                sample=(f"shot 0 ({sh.nx}x{survey.nz} window), {n_run} of {nt} steps per phase "
+                        f"(forward with snapshots + backward with imaging), FP32, P-SV+SH as the "
+                        f"reference runs, scaled x{nt / n_run:.1f} to one shot"))
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    survey = build_workload(3000)
+    import platform
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_rtm_sample(survey, target_s=4.0)
+        if i >= args.warmup:
+            vals.append(r["value"])
+    v = float(np.mean(vals))
+    line = dict(impl="reference", metric=METRIC, value=v, unit="shots/s", n_gpus=args.gpus,
+                steps=args.steps, warmup=args.warmup, ms_per_step=1000.0 / v * 1.0,
+                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
+                config=dict(workload=workload_desc(64, 3000) + " (per-shot rate on a bounded sample)",
+                            host=platform.processor() or platform.machine()),
+                cpu_baseline=dict(value=v, unit="shots/s", cores=r["cores"], kind="port", sample=r["sample"]),
+                e2e=dict(value=v, unit="shots/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+                note="Taichi (the reference's runtime) is not installable offline; the reference arm "
+                     "times the C/OpenMP restatement of its kernels on all host cores")
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- GPU
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nt", type=int, default=3000)
+    ap.add_argument("--shots", type=int, default=64)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-plain", action="store_true", help="skip the one-shot-per-launch leg")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank)
+
+    import torch
+    import torch.distributed as dist
+    from taichirtm_b200.batch import BatchedRTM, survey_shots, survey_wavelets
+    from taichirtm_b200.plan import PSV
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    survey = build_workload(args.nt)
+    survey.shots = survey.shots[: args.shots]
+    shots = survey_shots(survey)
+    wav = torch.as_tensor(survey_wavelets(survey)).to(dev)
+    mu_t, lam_t, rho_t = survey.material()
+    mu_m, lam_m, rho_m = survey.material(migration=True)
+
+    # observed data: forward on the true model (untimed)
+    true = BatchedRTM(mu_t, lam_t, rho_t, survey.dx, survey.dz, survey.fs, survey.nt, survey.fw, shots,
+                      modes=PSV, tune="auto", device=dev)
+    flags, obs, _, _ = true.forward(wav, save=False, check_interval=100)
+    assert int(flags.max()) == 0, flags
+    obs = obs.clone()
+    true.close()
+    del true
+    rtm = BatchedRTM(mu_m, lam_m, rho_m, survey.dx, survey.dz, survey.fs, survey.nt, survey.fw, shots,
+                     modes=PSV, tune="auto", device=dev)
+    plan = rtm.plan
+    cells = rtm.cells()
+    nt = survey.nt
+    nsnap = nt // ISNAP
+    n_img = sum(1 for t in range(1, nt) if t % ISNAP == 0 and t // ISNAP - 1 < nsnap)
+    stack = torch.zeros((3, survey.nx, survey.nz), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def one_step(ev=None):
+        if ev:
+            ev[0].record(stream)
+        ff, _, snaps, isnaps = plan.forward(wav, save=True, isnap=ISNAP, check_interval=100)
+        if ev:
+            ev[1].record(stream)
+        fb, _, _ = plan.backward(obs, snaps, isnaps, len(isnaps), ISNAP, check_interval=100, image=False,
+                                 stack=stack)
+        if ev:
+            ev[2].record(stream)
+        return ff, fb
+
+    for _ in range(args.warmup):
+        ff, fb = one_step()
+        assert int(ff.max()) == 0 and int(fb.max()) == 0
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler()
+    sampler.start()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    launches = 0
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t_start.record(stream)
+    for k in range(args.steps):
+        one_step(evs[k])
+        launches += plan.launch_count()  # backward launches
+        launches += nt + 1               # forward: nt step launches + seismogram transpose
+    if world > 1:
+        dist.all_reduce(stack)           # cross-GPU image stack (FP64)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop(os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0] or None)
+    ms = t_start.elapsed_time(t_end)
+    fwd_ms = sum(e[0].elapsed_time(e[1]) for e in evs)
+    bwd_ms = sum(e[1].elapsed_time(e[2]) for e in evs)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    shots_total = len(shots) * world * args.steps
+    value = shots_total / (ms / 1000.0)
+    gcell = 2.0 * cells * nt * world * args.steps / (ms / 1000.0) / 1e9
+
+    # roofline of the fused step kernels (forward + backward launches of the timed region)
+    alg_fwd = cells * (nt * BYTES_PER_CELL + (nsnap if nsnap * ISNAP <= nt - 1 else nsnap - 1) * SNAP_BYTES_PER_CELL)
+    alg_bwd = cells * (nt * BYTES_PER_CELL + n_img * IMG_BYTES_PER_CELL)
+    per_launch_bytes = (alg_fwd + alg_bwd) / (2 * nt)
+    per_launch_ms = (fwd_ms + bwd_ms) / args.steps / (2 * nt)
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    peak, peak_kind = peak_hbm()
+    tpc = ncu_traffic_per_cell()
+    roofline = dict(bound="hbm", achieved=round(achieved, 1), peak=peak, unit="GB/s",
+                    frac=round(achieved / peak, 4),
+                    traffic=(round(tpc * cells) if tpc else None),
+                    kernel="step_kernel<fwd|bwd, P-SV> (one launch = one time step of all shots)",
+                    bytes_per_launch=int(per_launch_bytes), us_per_launch=round(per_launch_ms * 1e3, 2),
+                    peak_source=peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind)
+
+    # end to end through the public API: host inputs, device outputs read back
+    wav_h = wav.cpu().pin_memory()
+    obs_h = obs.cpu().pin_memory()
+    h2d = wav_h.numel() * 4 + obs_h.numel() * 4
+    d2h = stack.numel() * 8
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        _, _, st = rtm.migrate(wav_h.to(dev, non_blocking=True), obs_h.to(dev, non_blocking=True),
+                               isnap=ISNAP, check_interval=100)
+        if world > 1:
+            dist.all_reduce(st)
+        host_img = st.cpu()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = dict(value=shots_total / (e2e_ms / 1000.0), unit="shots/s", h2d_bytes_per_step=int(h2d),
+               d2h_bytes_per_step=int(d2h), api="taichirtm_b200.batch.BatchedRTM.migrate")
+    assert np.isfinite(host_img.numpy()).all()
+
+    # the plain path: one shot per launch sequence, same shots, same semantics
+    plain = None
+    if not args.no_plain and rank == 0:
+        nplain = 4
+        t_sum = 0.0
+        for s in range(nplain):
+            sub = [shots[s]]
+            ns = len(sub[0].src)
+            o0 = sum(len(x.src) for x in shots[:s])
+            r0 = sum(len(x.rec) for x in shots[:s])
+            one = BatchedRTM(mu_m, lam_m, rho_m, survey.dx, survey.dz, survey.fs, nt, survey.fw, sub,
+                             modes=PSV, tune=dict(vec=2, rows=16, warps=4), device=dev)
+            w1 = wav[:, o0:o0 + ns].contiguous()
+            o1 = obs[:, r0:r0 + len(sub[0].rec)].contiguous()
+            one.migrate(w1, o1, isnap=ISNAP)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            one.migrate(w1, o1, isnap=ISNAP)
+            b.record(stream)
+            torch.cuda.synchronize()
+            t_sum += a.elapsed_time(b)
+            one.close()
+        plain = dict(shots_per_s=round(nplain / (t_sum / 1000.0), 3),
+                     sample=f"shots 0..{nplain - 1} migrated one shot per launch, per-step launches")
+
+    cpu = None
+    if not args.no_cpu and rank == 0 and world == 1:
+        cpu = cpu_rtm_sample(survey)
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = dict(
+            metric=METRIC, value=round(value, 4), unit="shots/s", n_gpus=world, steps=args.steps,
+            warmup=args.warmup, ms_per_step=round(ms_per_step, 2), higher_is_better=True, scaling="weak",
+            vs_baseline=None, dtype="f32", data="synthetic",
+            config=dict(workload=workload_desc(len(shots), nt), shots_per_gpu=len(shots),
+                        cells_per_shot_step=int(cells), grid="2001x801", nt=nt, isnap=ISNAP,
+                        l2="no flush: per-step working set (state 2.6 GB + snapshots 48 GB) >> 126 MB L2",
+                        parallelism=f"shots sharded, {len(shots)} per GPU, FP64 all-reduce of the image",
+                        launch_shape=rtm.tune),
+            gcell_upd_per_s=round(gcell, 2), roofline=roofline, e2e=e2e,
+            gpu_launches=int(launches), clocks=clocks, cpu_baseline=cpu)
+        if plain:
+            line["plain"] = plain
+            line["batched_vs_plain"] = round(value / world / plain["shots_per_s"], 2)
+        print(json.dumps(line), flush=True)
+    rtm.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

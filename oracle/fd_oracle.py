@@ -92,11 +92,20 @@ class _State:
 class Propagator:
     """One propagation phase on one grid: state, material, sponge, step kernels."""
 
-    def __init__(self, mu, lam, rho, dx, dz, fs, fw, surface=None, dtype=np.float64):
+    def __init__(self, mu, lam, rho, dx, dz, fs, fw, surface=None, dtype=np.float64, setup_f64=False):
         self.dtype = dtype
-        self.m = derived_material(mu, lam, rho, dtype)
-        self.nx, self.nz = self.m["mu"].shape
-        self.absorb = sponge(self.nx, self.nz, fw, dtype)
+        if setup_f64:
+            # one-time set-up evaluated in FP64 and rounded once to ``dtype``
+            # (the f32 4-point harmonic mean of fm:271 overflows for mu > ~4.3e9)
+            m64 = derived_material(np.asarray(mu, np.float32), np.asarray(lam, np.float32),
+                                   np.asarray(rho, np.float32), np.float64)
+            self.m = {k: v.astype(dtype) for k, v in m64.items()}
+            self.nx, self.nz = self.m["mu"].shape
+            self.absorb = sponge(self.nx, self.nz, fw, np.float64).astype(dtype)
+        else:
+            self.m = derived_material(mu, lam, rho, dtype)
+            self.nx, self.nz = self.m["mu"].shape
+            self.absorb = sponge(self.nx, self.nz, fw, dtype)
         self.surface = None if surface is None else np.asarray(surface, dtype)
         dt = 1.0 / float(fs)  # forward_modeling.py:135
         self.dt = _c(dt, dtype)
@@ -223,15 +232,16 @@ class Propagator:
 
 def forward(mu, lam, rho, dx, dz, nt, fs, fw, src, wu, wv, ww, rec, isnap=10,
             surface=None, save=False, check_interval=100, dtype=np.float64,
-            return_state=False):
+            return_state=False, setup_f64=False):
     """ForwardModeling.run, forward_modeling.py:504-575.
 
     Returns dict(flag, seis (3, nrec, nt), snaps (3, nx, nz, nsnap) or None,
     isnaps, num_snaps).  A non-zero flag returns at the failing check step,
     like the reference (the seismogram is filled up to that step).
     ``check_interval=0`` disables the finite check (used to compare with the
-    Taichi-stub golden runs, whose check cannot fire)."""
-    p = Propagator(mu, lam, rho, dx, dz, fs, fw, surface, dtype)
+    Taichi-stub golden runs, whose check cannot fire).  ``setup_f64`` evaluates
+    the one-time material set-up in FP64 (see Propagator)."""
+    p = Propagator(mu, lam, rho, dx, dz, fs, fw, surface, dtype, setup_f64)
     src = np.asarray(src).reshape(-1, 2)
     rec = np.asarray(rec).reshape(-1, 2)
     wu, wv, ww = (np.asarray(x, dtype).reshape(len(src), -1) for x in (wu, wv, ww))
@@ -273,12 +283,16 @@ def forward(mu, lam, rho, dx, dz, nt, fs, fw, src, wu, wv, ww, rec, isnap=10,
 
 
 def backward(mu, lam, rho, dx, dz, nt, fs, fw, rec, ou, ov, ow, snaps, isnaps, num_snaps,
-             isnap, surface=None, check_interval=100, dtype=np.float64, return_state=False):
+             isnap, surface=None, check_interval=100, dtype=np.float64, return_state=False,
+             setup_f64=False, kahan=False):
     """BackwardModeling.run_calc, backward_modeling.py:498-579.
 
     ``snaps`` is (3, nx, nz, nsnap) like the reference's snapshot fields.
+    ``kahan`` accumulates the image with Kahan compensation (sum, comp) and
+    returns sum - comp evaluated in FP64 then rounded to ``dtype``.
     Returns dict(flag, img (3, nx, nz))."""
-    p = Propagator(mu, lam, rho, dx, dz, fs, fw, surface, dtype)
+    p = Propagator(mu, lam, rho, dx, dz, fs, fw, surface, dtype, setup_f64)
+    comp = np.zeros((3, p.nx, p.nz), dtype)
     rec = np.asarray(rec).reshape(-1, 2)
     ou, ov, ow = (np.asarray(x, dtype) for x in (ou, ov, ow))
     img = np.zeros((3, p.nx, p.nz), dtype)
@@ -293,13 +307,21 @@ def backward(mu, lam, rho, dx, dz, nt, fs, fw, rec, ou, ov, ow, snaps, isnaps, n
         if t > 0 and t % isnap == 0:
             k = t // isnap - 1
             if 0 <= k < num_snaps and int(isnaps[k]) == t:
-                img[0] += snaps[0, :, :, k] * p.s.u
-                img[1] += snaps[1, :, :, k] * p.s.v
-                img[2] += snaps[2, :, :, k] * p.s.w
+                for c, f in enumerate((p.s.u, p.s.v, p.s.w)):
+                    prod = snaps[c, :, :, k] * f
+                    if kahan:
+                        y = prod - comp[c]
+                        tot = img[c] + y
+                        comp[c] = (tot - img[c]) - y
+                        img[c] = tot
+                    else:
+                        img[c] += prod
         if check_interval and it % check_interval == 0:
             flag = p.check_finite(4)
             if flag:
                 break
+    if kahan:
+        img = (img.astype(np.float64) - comp.astype(np.float64)).astype(dtype)
     out = dict(flag=flag, img=img)
     if return_state:
         out["state"] = p.s

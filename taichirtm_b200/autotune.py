@@ -1,0 +1,91 @@
+"""Launch-shape autotuner for the fused step kernels.
+
+The shape is (vec columns per lane, rows per warp task, warps per CTA).
+Results never depend on it (every cell's arithmetic is the same; FMA
+contraction is off), so the tuner only times: it builds a short plan for each
+candidate, times a few forward steps with CUDA events, and caches the best
+per (GPU, nz, total window rows, shots, modes) in a JSON file
+($TAICHIRTM_B200_CACHE or ~/.cache/taichirtm_b200/autotune.json)."""
+import json
+import os
+
+import torch
+
+CANDIDATES = [
+    dict(vec=2, rows=32, warps=4), dict(vec=4, rows=32, warps=4), dict(vec=2, rows=16, warps=4),
+    dict(vec=1, rows=16, warps=4), dict(vec=2, rows=64, warps=8), dict(vec=4, rows=16, warps=2),
+    dict(vec=1, rows=8, warps=4), dict(vec=2, rows=8, warps=2),
+]
+TUNE_STEPS = 24
+
+
+def _cache_path():
+    p = os.environ.get("TAICHIRTM_B200_CACHE")
+    if p:
+        return p
+    return os.path.join(os.path.expanduser("~"), ".cache", "taichirtm_b200", "autotune.json")
+
+
+def _load():
+    try:
+        with open(_cache_path()) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def _store(cache):
+    p = _cache_path()
+    try:
+        os.makedirs(os.path.dirname(p), exist_ok=True)
+        with open(p + ".tmp", "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+        os.replace(p + ".tmp", p)
+    except OSError:
+        pass
+
+
+def key(nz, shots, modes):
+    name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
+    rows = sum(s.nx for s in shots)
+    return f"{name}|nz={nz}|rows={rows}|shots={len(shots)}|modes={modes}"
+
+
+def time_shape(make_plan, shots, tune, steps=TUNE_STEPS):
+    import numpy as np
+    p = make_plan(tune, steps)
+    try:
+        nsrc = sum(len(s.src) for s in shots)
+        wav = torch.zeros((3, nsrc, steps), dtype=torch.float32, device=p.device)
+        if nsrc:
+            wav[:, :, 1] = 1.0
+        p.forward(wav, check_interval=0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        p.forward(wav, check_interval=0)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+    finally:
+        p.close()
+
+
+def best_shape(make_plan, nz, shots, modes, nt, candidates=None, refresh=False):
+    """Cached best launch shape; tunes on a miss."""
+    k = key(nz, shots, modes)
+    cache = _load()
+    if not refresh and k in cache:
+        return cache[k]["tune"]
+    results = []
+    for t in candidates or CANDIDATES:
+        try:
+            results.append((time_shape(make_plan, shots, t), t))
+        except Exception:
+            continue
+    if not results:
+        return None
+    ms, best = min(results, key=lambda r: r[0])
+    cache[k] = dict(tune=best, ms_per_step=ms, tried=[dict(t, ms=m) for m, t in results])
+    _store(cache)
+    return best

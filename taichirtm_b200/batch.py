@@ -1,0 +1,102 @@
+"""Batched RTM: many shots, each on its own window of one model, advanced
+together -- one kernel launch per time step covers every shot.
+
+The reference runs one shot per ``ReverseTimeMigration.run`` and sums the
+per-shot images afterwards (examples/example_2nd_step.py:102-158,
+src/imaging.py:81-93).  Here each shot keeps the reference's semantics on its
+window (a window behaves exactly like the reference run on the cropped model:
+sponge, edge cells and injection use the window's own edges), and the
+cross-shot sum is an FP64 reduction on the GPU."""
+from typing import List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import autotune
+from .fields import to_tensor
+from .plan import PSV, SH, Plan, ShotGeometry, require_cuda
+
+
+class BatchedRTM:
+    """Many shots on one model.
+
+    mu, lam, rho : (nx, nz) model (the reference's mu/lam/rho fields).
+    shots        : ShotGeometry list (window rows and LOCAL source/receiver
+                   grid indices).
+    modes        : PSV, SH or BOTH (default PSV).
+    tune         : launch shape dict, "auto" (autotuner, cached), or None.
+    """
+
+    def __init__(self, mu, lam, rho, dx, dz, fs, nt, absorbing_frame, shots: Sequence[ShotGeometry],
+                 modes=PSV, surface=None, tune="auto", device=None):
+        require_cuda()
+        self.device = torch.device(device if device is not None else "cuda")
+        self.nx, self.nz = tuple(np.shape(mu))
+        self.dx, self.dz, self.fs, self.nt = float(dx), float(dz), float(fs), int(nt)
+        self.fw = int(absorbing_frame)
+        self.modes = int(modes)
+        self.shots: List[ShotGeometry] = list(shots)
+        self._model = [to_tensor(x, torch.float32, self.device) for x in (mu, lam, rho)]
+        self._surface = None if surface is None else to_tensor(surface, torch.float32, self.device)
+        if tune == "auto":
+            tune = autotune.best_shape(self._make_plan, self.nz, self.shots, self.modes, self.nt)
+        self.tune = tune
+        self.plan = self._make_plan(tune, self.nt)
+
+    def _make_plan(self, tune, nt):
+        p = Plan(self.nx, self.nz, self.dx, self.dz, nt, self.fs, self.fw, self.modes, self.shots,
+                 tune=tune, device=self.device)
+        p.set_model(*self._model, self._surface)
+        return p
+
+    @property
+    def nsrc_total(self):
+        return self.plan.nsrc_total
+
+    @property
+    def nrec_total(self):
+        return self.plan.nrec_total
+
+    def cells(self):
+        return sum(s.nx for s in self.shots) * self.nz
+
+    def forward(self, wavelets, save=False, isnap=10, check_interval=100):
+        """wavelets (3, nsrc_total, nt) -> (flags, seismograms (3, nrec_total, nt),
+        snapshot buffers, isnaps)."""
+        w = to_tensor(wavelets, torch.float32, self.device)
+        return self.plan.forward(w, save=save, isnap=isnap, check_interval=check_interval)
+
+    def migrate(self, wavelets, observed, isnap=10, check_interval=100, stack=None):
+        """Forward with snapshots, backward with imaging, FP64 stack of every
+        shot's image on the global grid.  Returns (forward flags, backward
+        flags, stack (3, nx, nz) float64 on the device)."""
+        w = to_tensor(wavelets, torch.float32, self.device)
+        o = to_tensor(observed, torch.float32, self.device)
+        ff, _, snaps, isnaps = self.plan.forward(w, save=True, isnap=isnap, check_interval=check_interval)
+        if stack is None:
+            stack = torch.zeros((3, self.nx, self.nz), dtype=torch.float64, device=self.device)
+        fb, _, _ = self.plan.backward(o, snaps, isnaps, len(isnaps), isnap, check_interval=check_interval,
+                                      image=False, stack=stack)
+        del snaps
+        return ff, fb, stack
+
+    def launch_count(self):
+        return self.plan.launch_count()
+
+    def close(self):
+        if self.plan is not None:
+            self.plan.close()
+            self.plan = None
+
+
+def survey_shots(survey) -> List[ShotGeometry]:
+    """ShotGeometry list of a taichirtm_b200.synthetic.Survey."""
+    return [ShotGeometry(s.x0, s.nx, s.src, s.rec) for s in survey.shots]
+
+
+def survey_wavelets(survey) -> np.ndarray:
+    return np.concatenate([s.wavelets for s in survey.shots], axis=1)
+
+
+def modes_of(name: Optional[str]):
+    return {"psv": PSV, "sh": SH, "both": PSV | SH}[name or "psv"]

@@ -379,6 +379,20 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
     }
     cudaStream_t s = (cudaStream_t)stream;
     if (int rc = zero_state(p, s)) return rc;
+    // Snapshot slots the time loop never reaches ((k+1)*isnap > nt-1) stay
+    // zero, like the reference's zero-initialised fields (fm:533-535).
+    if (save)
+        for (int k = 0; k < nsnap; ++k) {
+            if ((long long)(k + 1) * isnap <= nt - 1) continue;
+            float *sp3[3] = {snap_u, snap_v, snap_w};
+            for (int c = 0; c < 3; ++c) {
+                if (!comp_active(p->g.modes, c) || !sp3[c]) continue;
+                for (const ShotDev &d : p->shots_h) {
+                    const size_t off = ((size_t)nsnap * d.row_off + (size_t)k * d.nx) * p->pitch;
+                    CUDA_TRY(cudaMemsetAsync(sp3[c] + off, 0, (size_t)d.nx * p->pitch * sizeof(float), s));
+                }
+            }
+        }
     const size_t nseis = (size_t)3 * nt * p->nrec_total;
     if (nseis) CUDA_TRY(cudaMemsetAsync(p->d_seis_t, 0, nseis * sizeof(float), s));
     StepParams sp;

@@ -167,6 +167,36 @@ def test_launch_shapes_agree(tune):
     assert np.array_equal(out[0][1], out[1][1])
 
 
+@pytest.mark.parametrize("name", ["fwbw_basic", "fwbw_topo"])
+def test_bit_exact_vs_fp32_restatement(name):
+    """With FMA contraction off, each cell's FP32 arithmetic on the GPU is the
+    reference's expression order; the NumPy FP32 restatement with the same
+    one-time FP64 set-up and Kahan imaging gives identical bits."""
+    from oracle import fd_oracle
+    from taichirtm_b200.plan import Plan, ShotGeometry
+    g = load_golden(name)
+    sm = g["surface"] if g["surface"].size else None
+    nx, nz, nt, isnap = int(g["nx"]), int(g["nz"]), int(g["nt"]), int(g["isnap"])
+    kw = dict(dx=float(g["dx"]), dz=float(g["dz"]), nt=nt, fs=float(g["fs"]), fw=int(g["fw"]))
+    ref = fd_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], src=g["src"], wu=g["wu"], wv=g["wv"],
+                            ww=g["ww"], rec=g["rec"], isnap=isnap, surface=sm, save=True,
+                            dtype=np.float32, setup_f64=True, **kw)
+    bref = fd_oracle.backward(g["mu_s"], g["lam_s"], g["rho_s"], rec=g["rec"], ou=g["obs"][0],
+                              ov=g["obs"][1], ow=g["obs"][2], snaps=ref["snaps"], isnaps=ref["isnaps"],
+                              num_snaps=ref["num_snaps"], isnap=isnap, surface=sm, dtype=np.float32,
+                              setup_f64=True, kahan=True, **kw)
+    p = Plan(nx, nz, kw["dx"], kw["dz"], nt, kw["fs"], kw["fw"], 3, [ShotGeometry(0, nx, g["src"], g["rec"])])
+    p.set_model(g["mu_s"], g["lam_s"], g["rho_s"], sm)
+    f, seis, snaps, isn = p.forward(torch.as_tensor(np.stack([g["wu"], g["wv"], g["ww"]])), save=True,
+                                    isnap=isnap)
+    assert np.array_equal(seis.cpu().numpy(), ref["seis"])
+    for c in range(3):
+        assert np.array_equal(p.snapshot_view(snaps[c], len(isn)).cpu().numpy(), ref["snaps"][c])
+    f2, img, _ = p.backward(torch.as_tensor(g["obs"]).float(), snaps, isn, len(isn), isnap)
+    assert np.array_equal(img.cpu().numpy(), bref["img"])
+    p.close()
+
+
 @pytest.mark.parametrize("name", ["rtm_vfix", "rtm_vscan_topo"])
 def test_reverse_time_migration_run_golden(name):
     """ReverseTimeMigration.run end to end (rtm.py:846-1029) vs the reference
