@@ -1,0 +1,311 @@
+// Exact discrete adjoint of the P-SV forward step (no counterpart in the
+// reference, whose backward propagation is neither the adjoint nor the time
+// reverse of its forward: it uses -dt with transposed difference directions,
+// src/backward_modeling.py:312-380).
+//
+// Forward step n in stored quantities (V = (u, w), S = (sxx, szz, sxz), I =
+// interior mask, c = sponge, m = surface mask on sxz/szz, B = (inv_rho_u,
+// inv_rho_w), Dv = backward differences of the velocity update, Ds = forward
+// differences of the stress update, C = (lam, mu, mxz)):
+//   v'_n = V_{n-1} + I dt B Dv(S_{n-1}) + src_n                      (fm:330-347, 421-443)
+//   s'_n = S_{n-1} + I dt C(Ds(v'_n))                                (fm:367-384)
+//   V_n  = c v'_n,   S_n = c m s'_n                                  (fm:386-419)
+//   d_n  = R V_n                                                     (fm:445-453)
+// Its adjoint, with a_n = dJ/dV_n and b_n = dJ/dS_n:
+//   beta'  = c m b_n,      beta = I beta'
+//   ubar   = dt C^T beta   (adjoint strain rates u_x, w_z and u_z = w_x)
+//   alpha' = c a_n + Ds^T ubar                    (= dJ/dv'_n)
+//   gamma  = I dt B alpha'
+//   b_{n-1} = beta' + Dv^T gamma,   a_{n-1} = alpha' + R^T g_{n-1}
+// and the model gradients accumulated over n:
+//   dJ/dlam += dt (beta_xx + beta_zz) div(v'_n),  dJ/dmu += 2 dt (beta_xx u_x + beta_zz w_z),
+//   dJ/dmxz += dt beta_xz (u_z + w_x),            dJ/dB   += alpha' I dt Dv(S_{n-1})
+//                                                           (+ alpha' w_n f at interior sources),
+// and dJ/dw_n = alpha'(src) f B(src) for the wavelets.
+//
+// One launch reverses step n for every shot.  Rows stream like the forward
+// kernel: lanes 1..30 own VEC columns each, lanes 0 / 31 are the column halo,
+// and row r = k-1 is finished while row k streams in, so every neighbour is in
+// a register or one shuffle away.  v'_n is recomputed on the fly from the
+// stored forward state n-1.
+#pragma once
+#include "step_kernels.cuh"
+
+namespace rtm {
+
+enum AdjField { A_U = 0, A_W, A_SXX, A_SZZ, A_SXZ, NADJ };
+enum Grad { G_LAM = 0, G_MU, G_MXZ, G_BU, G_BW, NGRAD };
+
+struct AdjParams {
+    int nz, pitch, nt, fw;
+    float dt, inv_dx, inv_dz, src_factor;
+    const float *sponge;
+    const int4 *work;
+    int n_work;
+    const ShotDev *shots;
+    const float *fwd[NADJ];   // forward state n-1 (stored, absorbed): u, w, sxx, szz, sxz
+    const float *ain[NADJ];   // adjoint state n
+    float *aout[NADJ];        // adjoint state n-1
+    const float *mat[NMAT];
+    const float *surface;
+    const int *src_ptr;
+    const int2 *src_ent;
+    const float *wav[3];      // (nsrc_total, nt)
+    const int *rec_ptr;
+    const int2 *rec_ent;
+    int nrec_total;
+    const float *resid[3];    // time-major (nt, nrec_total): dJ/d(seismogram)
+    float *grad[NGRAD];       // per shot [row_off + i][pitch], Kahan sums
+    float *gradc[NGRAD];      // Kahan compensations
+    float *gwav[3];           // time-major (nt, nsrc_total) dJ/d(wavelet), or null
+    int nsrc_total;
+    int n;                    // forward step reversed by this launch
+};
+
+// Same coefficient as sponge_coef (forward_modeling.py:203-235 loop order).
+__device__ __forceinline__ float adj_sponge(const float *prof, int fw, int nz, int nx, int i, int j) {
+    const int db = nz - 1 - j, dr = nx - 1 - i;
+    int d = -1;
+    if (i >= 0 && i < fw && db > i) d = i;
+    if (dr >= 0 && dr < fw && db > dr) d = dr;
+    if (db >= 0 && db < fw && i >= db && dr >= db) d = db;
+    return d >= 0 ? __ldg(prof + d) : 1.0f;
+}
+
+template <int VEC>
+__global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
+    constexpr int W = 30 * VEC;
+    const int lane = threadIdx.x & 31;
+    const int task = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (task >= p.n_work) return;
+    const int4 wk = p.work[task];
+    const ShotDev sh = p.shots[wk.x];
+    const int nx = sh.nx, nz = p.nz, P = p.pitch;
+    const int c0 = wk.y * W - VEC + VEC * lane;
+    const bool owner = lane >= 1 && lane <= 30;
+    const int ia = wk.z, ib = wk.w;
+    const long long soff = sh.state_off + (long long)(c0 + COL_OFF);
+    const long long moff = (long long)sh.x0 * P + (long long)(c0 + COL_OFF);
+    const float dt = p.dt, idx = p.inv_dx, idz = p.inv_dz;
+    const int n = p.n;
+    auto F = [&](int f, int i) { return p.fwd[f] + soff + (long long)(i + 1) * P; };
+    auto A = [&](int f, int i) { return p.ain[f] + soff + (long long)(i + 1) * P; };
+    auto M = [&](int m, int i) { return p.mat[m] + moff + (long long)(i + 1) * P; };
+
+    // row k-1 registers
+    float sxx_p[VEC], sxz_p[VEC], szz_p[VEC];  // forward stress
+    float uxb_p[VEC], wzb_p[VEC], xzb_p[VEC];  // adjoint strain rates
+    float bxx_p[VEC], bzz_p[VEC], bxz_p[VEC];  // beta'
+    float ins_p[VEC];                          // interior mask (1/0)
+    float up_p[VEC], wp_p[VEC];                // v'_n
+    float au_p[VEC], aw_p[VEC];                // alpha'
+    float gu_p[VEC], gw_p[VEC];                // gamma
+    float dvu_p[VEC], dvw_p[VEC];              // Dv(S_{n-1})
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+        sxx_p[q] = sxz_p[q] = szz_p[q] = 0.f;
+        uxb_p[q] = wzb_p[q] = xzb_p[q] = 0.f;
+        bxx_p[q] = bzz_p[q] = bxz_p[q] = 0.f;
+        ins_p[q] = 0.f;
+        up_p[q] = wp_p[q] = au_p[q] = aw_p[q] = gu_p[q] = gw_p[q] = dvu_p[q] = dvw_p[q] = 0.f;
+    }
+
+    for (int k = ia - 1; k <= ib; ++k) {
+        // ---- pointwise quantities of row k
+        float sxx[VEC], szz[VEC], sxz[VEC], bxx[VEC], bzz[VEC], bxz[VEC];
+        float lam[VEC], mu[VEC], mxz[VEC], sm[VEC];
+        ldv<VEC>(sxx, F(A_SXX, k));
+        ldv<VEC>(szz, F(A_SZZ, k));
+        ldv<VEC>(sxz, F(A_SXZ, k));
+        ldv<VEC>(bxx, A(A_SXX, k));
+        ldv<VEC>(bzz, A(A_SZZ, k));
+        ldv<VEC>(bxz, A(A_SXZ, k));
+        ldv<VEC>(lam, M(M_LAM, k));
+        ldv<VEC>(mu, M(M_MU, k));
+        ldv<VEC>(mxz, M(M_MXZ, k));
+        if (p.surface) {
+            ldv<VEC>(sm, p.surface + moff + (long long)(k + 1) * P);
+        } else {
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) sm[q] = 1.f;
+        }
+        float cc[VEC], ins[VEC], uxb[VEC], wzb[VEC], xzb[VEC];
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            const int j = c0 + q;
+            cc[q] = adj_sponge(p.sponge, p.fw, nz, nx, k, j);
+            ins[q] = interior(k, j, nx, nz) ? 1.f : 0.f;
+            bxx[q] = cc[q] * bxx[q];                 // beta' = c m b
+            bzz[q] = (cc[q] * bzz[q]) * sm[q];
+            bxz[q] = (cc[q] * bxz[q]) * sm[q];
+            const float Bxx = ins[q] != 0.f ? bxx[q] : 0.f;  // beta = I beta'
+            const float Bzz = ins[q] != 0.f ? bzz[q] : 0.f;
+            const float Bxz = ins[q] != 0.f ? bxz[q] : 0.f;
+            const float l2m = lam[q] + 2.0f * mu[q];
+            uxb[q] = dt * (l2m * Bxx + lam[q] * Bzz);
+            wzb[q] = dt * (lam[q] * Bxx + l2m * Bzz);
+            xzb[q] = dt * (mxz[q] * Bxz);
+        }
+        float up[VEC], wp[VEC], au[VEC], aw[VEC], gu[VEC], gw[VEC], dvu[VEC], dvw[VEC];
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) up[q] = wp[q] = au[q] = aw[q] = gu[q] = gw[q] = dvu[q] = dvw[q] = 0.f;
+        // column j-1 neighbours of row k
+        const float sxz_m = __shfl_up_sync(FULL, sxz[VEC - 1], 1);
+        const float szz_m = __shfl_up_sync(FULL, szz[VEC - 1], 1);
+        const float xzb_m = __shfl_up_sync(FULL, xzb[VEC - 1], 1);
+        const float wzb_m = __shfl_up_sync(FULL, wzb[VEC - 1], 1);
+        if (k >= ia) {
+            float u[VEC], w[VEC], bu[VEC], bw[VEC], au_in[VEC], aw_in[VEC];
+            ldv<VEC>(u, F(A_U, k));
+            ldv<VEC>(w, F(A_W, k));
+            ldv<VEC>(au_in, A(A_U, k));
+            ldv<VEC>(aw_in, A(A_W, k));
+            ldv<VEC>(bu, M(M_IRU, k));
+            ldv<VEC>(bw, M(M_IRW, k));
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                const float sxz_jm = q > 0 ? sxz[q - 1] : sxz_m;
+                const float szz_jm = q > 0 ? szz[q - 1] : szz_m;
+                const float xzb_jm = q > 0 ? xzb[q - 1] : xzb_m;
+                const float wzb_jm = q > 0 ? wzb[q - 1] : wzb_m;
+                // forward recompute of v'_n (fm:332-340)
+                dvu[q] = (sxx[q] - sxx_p[q]) * idx + (sxz[q] - sxz_jm) * idz;
+                dvw[q] = (sxz[q] - sxz_p[q]) * idx + (szz[q] - szz_jm) * idz;
+                const bool in = ins[q] != 0.f;
+                up[q] = in ? u[q] + dvu[q] * dt * bu[q] : u[q];
+                wp[q] = in ? w[q] + dvw[q] * dt * bw[q] : w[q];
+                // alpha' = c a + Ds^T ubar
+                au[q] = cc[q] * au_in[q] + (uxb_p[q] - uxb[q]) * idx + (xzb_jm - xzb[q]) * idz;
+                aw[q] = cc[q] * aw_in[q] + (xzb_p[q] - xzb[q]) * idx + (wzb_jm - wzb[q]) * idz;
+                gu[q] = in ? dt * bu[q] * au[q] : 0.f;
+                gw[q] = in ? dt * bw[q] * aw[q] : 0.f;
+            }
+            // sources of row k: recompute injection (fm:421-443)
+            if (k < nx && n < p.nt) {
+                const int e0 = __ldg(p.src_ptr + sh.src_row0 + k), e1 = __ldg(p.src_ptr + sh.src_row0 + k + 1);
+                for (int e = e0; e < e1; ++e) {
+                    const int2 en = __ldg(p.src_ent + e);
+                    const int q = en.x - c0;
+                    if (q < 0 || q >= VEC) continue;
+                    const bool in = interior(k, en.x, nx, nz);
+                    const size_t t = (size_t)en.y * p.nt + n;
+#pragma unroll
+                    for (int qq = 0; qq < VEC; ++qq) {
+                        if (qq != q) continue;
+                        up[qq] += __ldg(p.wav[0] + t) * p.src_factor * (in ? bu[qq] : __int_as_float(0x7f800000));
+                        wp[qq] += __ldg(p.wav[2] + t) * p.src_factor * (in ? bw[qq] : __int_as_float(0x7f800000));
+                    }
+                }
+            }
+        }
+        if (k >= ia + 1) {
+            // ---- finish row r = k-1
+            const int r = k - 1;
+            const float gu_n = __shfl_down_sync(FULL, gu_p[0], 1);  // gamma(r, j+1)
+            const float gw_n = __shfl_down_sync(FULL, gw_p[0], 1);
+            const float up_n = __shfl_down_sync(FULL, up_p[0], 1);  // v'(r, j+1)
+            const float wp_n = __shfl_down_sync(FULL, wp_p[0], 1);
+            float oxx[VEC], ozz[VEC], oxz[VEC], ou[VEC], ow[VEC];
+            float dl[VEC], dm[VEC], dxz[VEC], dbu[VEC], dbw[VEC];
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) {
+                const float gu_j = q < VEC - 1 ? gu_p[q + 1] : gu_n;
+                const float gw_j = q < VEC - 1 ? gw_p[q + 1] : gw_n;
+                const float up_j = q < VEC - 1 ? up_p[q + 1] : up_n;
+                const float wp_j = q < VEC - 1 ? wp_p[q + 1] : wp_n;
+                // b_{n-1} = beta' + Dv^T gamma
+                oxx[q] = bxx_p[q] + (gu_p[q] - gu[q]) * idx;
+                oxz[q] = bxz_p[q] + (gu_p[q] - gu_j) * idz + (gw_p[q] - gw[q]) * idx;
+                ozz[q] = bzz_p[q] + (gw_p[q] - gw_j) * idz;
+                ou[q] = au_p[q];
+                ow[q] = aw_p[q];
+                // gradients from v'_n (fm:369-378) and Dv(S_{n-1})
+                const float u_x = (up[q] - up_p[q]) * idx;
+                const float u_z = (up_j - up_p[q]) * idz;
+                const float w_x = (wp[q] - wp_p[q]) * idx;
+                const float w_z = (wp_j - wp_p[q]) * idz;
+                const bool in = ins_p[q] != 0.f;
+                const float Bxx = in ? bxx_p[q] : 0.f, Bzz = in ? bzz_p[q] : 0.f, Bxz = in ? bxz_p[q] : 0.f;
+                dl[q] = dt * ((Bxx + Bzz) * (u_x + w_z));
+                dm[q] = dt * (2.0f * (Bxx * u_x + Bzz * w_z));
+                dxz[q] = dt * (Bxz * (u_z + w_x));
+                dbu[q] = in ? au_p[q] * (dt * dvu_p[q]) : 0.f;
+                dbw[q] = in ? aw_p[q] * (dt * dvw_p[q]) : 0.f;
+            }
+            if (owner) {
+                // sources of row r: gradient of the injection scale and wavelet gradient
+                const int e0 = n < p.nt ? __ldg(p.src_ptr + sh.src_row0 + r) : 0;
+                const int e1 = n < p.nt ? __ldg(p.src_ptr + sh.src_row0 + r + 1) : 0;
+                for (int e = e0; e < e1; ++e) {
+                    const int2 en = __ldg(p.src_ent + e);
+                    const int q = en.x - c0;
+                    if (q < 0 || q >= VEC) continue;
+                    const bool in = interior(r, en.x, nx, nz);
+                    const size_t t = (size_t)en.y * p.nt + n;
+                    const float f = p.src_factor;
+#pragma unroll
+                    for (int qq = 0; qq < VEC; ++qq) {
+                        if (qq != q || !in) continue;
+                        dbu[qq] += au_p[qq] * (__ldg(p.wav[0] + t) * f);
+                        dbw[qq] += aw_p[qq] * (__ldg(p.wav[2] + t) * f);
+                        if (p.gwav[0]) {
+                            const float bu_r = __ldg(M(M_IRU, r) + qq), bw_r = __ldg(M(M_IRW, r) + qq);
+                            const size_t g = (size_t)n * p.nsrc_total + en.y;
+                            p.gwav[0][g] += au_p[qq] * f * bu_r;
+                            p.gwav[2][g] += aw_p[qq] * f * bw_r;
+                        }
+                    }
+                }
+                // R^T g_{n-1}: adjoint source at the receivers (fm:445-453 transposed)
+                if (n >= 1) {
+                    const int e0r = __ldg(p.rec_ptr + sh.rec_row0 + r), e1r = __ldg(p.rec_ptr + sh.rec_row0 + r + 1);
+                    for (int e = e0r; e < e1r; ++e) {
+                        const int2 en = __ldg(p.rec_ent + e);
+                        const int q = en.x - c0;
+                        if (q < 0 || q >= VEC) continue;
+                        const size_t t = (size_t)(n - 1) * p.nrec_total + en.y;
+#pragma unroll
+                        for (int qq = 0; qq < VEC; ++qq) {
+                            if (qq != q) continue;
+                            ou[qq] += __ldg(p.resid[0] + t);
+                            ow[qq] += __ldg(p.resid[2] + t);
+                        }
+                    }
+                }
+                const long long so = soff + (long long)(r + 1) * P;
+                stv<VEC>(p.aout[A_U] + so, ou);
+                stv<VEC>(p.aout[A_W] + so, ow);
+                stv<VEC>(p.aout[A_SXX] + so, oxx);
+                stv<VEC>(p.aout[A_SZZ] + so, ozz);
+                stv<VEC>(p.aout[A_SXZ] + so, oxz);
+                const long long go = (sh.row_off + r) * (long long)P + c0 + COL_OFF;
+                auto acc = [&](int gi, const float (&d)[VEC]) {
+                    float s[VEC], cmp[VEC];
+                    ldv<VEC>(s, p.grad[gi] + go);
+                    ldv<VEC>(cmp, p.gradc[gi] + go);
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) kahan_add(s[q], cmp[q], d[q]);
+                    stv<VEC>(p.grad[gi] + go, s);
+                    stv<VEC>(p.gradc[gi] + go, cmp);
+                };
+                acc(G_LAM, dl);
+                acc(G_MU, dm);
+                acc(G_MXZ, dxz);
+                acc(G_BU, dbu);
+                acc(G_BW, dbw);
+            }
+        }
+        // ---- shift row k into the row k-1 registers
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            sxx_p[q] = sxx[q]; sxz_p[q] = sxz[q]; szz_p[q] = szz[q];
+            uxb_p[q] = uxb[q]; wzb_p[q] = wzb[q]; xzb_p[q] = xzb[q];
+            bxx_p[q] = bxx[q]; bzz_p[q] = bzz[q]; bxz_p[q] = bxz[q];
+            ins_p[q] = ins[q];
+            up_p[q] = up[q]; wp_p[q] = wp[q]; au_p[q] = au[q]; aw_p[q] = aw[q];
+            gu_p[q] = gu[q]; gw_p[q] = gw[q]; dvu_p[q] = dvu[q]; dvw_p[q] = dvw[q];
+        }
+    }
+}
+
+}  // namespace rtm
