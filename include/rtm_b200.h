@@ -133,6 +133,30 @@ int rtm_backward(rtm_plan *plan, const float *obs, const float *snap_u, const fl
                  float *image, double *stack, int check_interval, int32_t *flags,
                  rtm_stream_t stream);
 
+/* Forward propagation of ONE shot on the whole grid that allocates no device
+ * memory.  No counterpart in the reference: it exists for callers that cannot
+ * call cudaMalloc while running, such as a plugin inside a host processing
+ * system that owns all device memory and hands the plugin only a stream and
+ * its buffers.  Inputs and outputs are the caller's: mu, lam, rho (nx, nz),
+ * wavelets (3, nsrc, nt), seis (3, nrec, nt), all device pointers; src_ij /
+ * rec_ij and *flag (status 0 / 1..3) are host memory.  Every intermediate
+ * lives in one static device array of rtm_noalloc_scratch_bytes() bytes
+ * (64 MiB, held by every GPU that loads the library until the process exits);
+ * a problem needing more (rtm_noalloc_required_bytes) is rejected with
+ * RTM_E_RANGE and a message.  The first call on a device looks up that array's
+ * device address; make that first call before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU (other streams, other host
+ * threads) race and must not be issued.  The call synchronises the stream.
+ * Results equal rtm_forward's on a one-shot full-grid plan (launch shape vec 2,
+ * 16 rows, 4 warps).  Errors: rtm_noalloc_last_error(). */
+int rtm_forward_noalloc(const rtm_grid *grid, int nsrc, const int32_t *src_ij, int nrec,
+                        const int32_t *rec_ij, const float *mu, const float *lam, const float *rho,
+                        const float *wavelets, float *seis, int check_interval, int32_t *flag,
+                        rtm_stream_t stream);
+size_t rtm_noalloc_scratch_bytes(void);
+size_t rtm_noalloc_required_bytes(const rtm_grid *grid, int nsrc, int nrec);
+const char *rtm_noalloc_last_error(void);
+
 /* Diagnostics: kernels launched by the last propagate call, and the last
  * error message of this thread. */
 long long rtm_plan_launch_count(const rtm_plan *plan);

@@ -14,7 +14,7 @@ namespace rtm {
 // inv_rho_u / inv_rho_w are +inf on the edge cells exactly as in the
 // reference.  mu, lam, rho: (nx, nz) contiguous.  Null outputs are skipped
 // (fields of a mode the plan does not propagate).
-__global__ void setup_material_kernel(const float *__restrict__ mu, const float *__restrict__ lam,
+static __global__ void setup_material_kernel(const float *__restrict__ mu, const float *__restrict__ lam,
                                       const float *__restrict__ rho, const float *__restrict__ surface,
                                       int nx, int nz, int pitch, float *iru, float *irw, float *olam,
                                       float *omu, float *mxz, float *ir, float *myx, float *myz,
@@ -50,7 +50,7 @@ __global__ void setup_material_kernel(const float *__restrict__ mu, const float 
 }
 
 // (rows, cols) -> (cols, rows) for `planes` stacked matrices.
-__global__ void transpose_kernel(const float *__restrict__ in, float *__restrict__ out, int rows,
+static __global__ void transpose_kernel(const float *__restrict__ in, float *__restrict__ out, int rows,
                                  int cols) {
     __shared__ float tile[32][33];
     const size_t plane = (size_t)rows * cols;
@@ -70,7 +70,7 @@ __global__ void transpose_kernel(const float *__restrict__ in, float *__restrict
 }
 
 // Per-shot Kahan image (sum, comp) -> compact (nx, nz) float image of one shot.
-__global__ void image_out_kernel(const float *__restrict__ sum, const float *__restrict__ comp,
+static __global__ void image_out_kernel(const float *__restrict__ sum, const float *__restrict__ comp,
                                  float *__restrict__ out, long long row_off, int nx, int nz,
                                  int pitch) {
     const long long n = (long long)nx * nz;
@@ -85,7 +85,7 @@ __global__ void image_out_kernel(const float *__restrict__ sum, const float *__r
 // Cross-shot sum in FP64 on the global grid (imaging.py:81-93 generalised to
 // windows): stack[x, j] += sum over shots covering row x of their image, in
 // shot order (deterministic).
-__global__ void stack_kernel(const float *__restrict__ sum, const float *__restrict__ comp,
+static __global__ void stack_kernel(const float *__restrict__ sum, const float *__restrict__ comp,
                              double *__restrict__ stack, const ShotDev *__restrict__ shots,
                              int nshots, int nx_g, int nz, int pitch) {
     const long long n = (long long)nx_g * nz;
