@@ -133,6 +133,34 @@ int rtm_backward(rtm_plan *plan, const float *obs, const float *snap_u, const fl
                  float *image, double *stack, int check_interval, int32_t *flags,
                  rtm_stream_t stream);
 
+/* ---- Exact adjoint (FWI gradients).  No counterpart in the reference, whose
+ * backward propagation (backward_modeling.py:312-380) is not the adjoint of
+ * its forward; these differentiate the forward step of
+ * forward_modeling.py:309-453 exactly.  P-SV plans only. */
+
+/* Floats of one wavefield component buffer of the plan (all shots, padded);
+ * a checkpoint slot holds 5 of them (u, w, sxx, szz, sxz). */
+size_t rtm_plan_state_floats(const rtm_plan *plan);
+/* Checkpoint slots for interval ckpt_every: ceil(nt / ckpt_every) - 1. */
+int rtm_plan_num_checkpoints(const rtm_plan *plan, int ckpt_every);
+
+/* ForwardModeling.run without snapshots (forward_modeling.py:504-575) that
+ * also stores the full state after every step it with (it+1) % ckpt_every == 0
+ * into ckpt (rtm_plan_num_checkpoints slots of 5 * rtm_plan_state_floats
+ * floats).  Storing costs no extra traffic: the step writes its output there. */
+int rtm_forward_checkpointed(rtm_plan *plan, const float *wavelets, float *seis, int ckpt_every,
+                             float *ckpt, int check_interval, int32_t *flags, rtm_stream_t stream);
+
+/* Adjoint sweep: given resid = dJ/d(seis) (3, nrec_total, nt) and the
+ * checkpoints of rtm_forward_checkpointed, recompute each segment forward and
+ * run the exact adjoint step backward through it.  Adds, per shot window, the
+ * gradients dJ/d(lam, mu, mxz, inv_rho_u, inv_rho_w) into grad
+ * ((5, nx, nz) float64, global grid; the caller zeroes it) and, if non-NULL,
+ * writes dJ/d(wavelets) into grad_wavelet (3, nsrc_total, nt).  Image-style
+ * Kahan FP32 accumulation per shot, FP64 sum over shots.  Synchronises. */
+int rtm_adjoint(rtm_plan *plan, const float *wavelets, const float *resid, int ckpt_every,
+                const float *ckpt, double *grad, float *grad_wavelet, rtm_stream_t stream);
+
 /* Forward propagation of ONE shot on the whole grid that allocates no device
  * memory.  No counterpart in the reference: it exists for callers that cannot
  * call cudaMalloc while running, such as a plugin inside a host processing

@@ -70,6 +70,10 @@ def lib():
     _sig(L, "rtm_plan_set_model", c_int, vp, vp, vp, vp, vp, vp)
     _sig(L, "rtm_forward", c_int, vp, vp, vp, c_int, c_int, vp, vp, vp, I32P, c_int, I32P, vp)
     _sig(L, "rtm_backward", c_int, vp, vp, vp, vp, vp, I32P, c_int, c_int, vp, vp, c_int, I32P, vp)
+    _sig(L, "rtm_plan_state_floats", c_size, vp)
+    _sig(L, "rtm_plan_num_checkpoints", c_int, vp, c_int)
+    _sig(L, "rtm_forward_checkpointed", c_int, vp, vp, vp, c_int, vp, c_int, I32P, vp)
+    _sig(L, "rtm_adjoint", c_int, vp, vp, vp, c_int, vp, vp, vp, vp)
     for name, args in _OPTIONAL.items():
         if hasattr(L, name):
             _sig(L, name, *args)

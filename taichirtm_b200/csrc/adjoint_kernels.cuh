@@ -62,6 +62,29 @@ struct AdjParams {
     int n;                    // forward step reversed by this launch
 };
 
+// Initial adjoint state a_{nt-1} = R^T g_{nt-1}: one thread per shot adds the
+// last residual sample at its receivers, in receiver order (duplicates at one
+// cell accumulate deterministically).  resid_t is time-major, 3 planes of
+// (nt, nrec_total).
+static __global__ void inject_last_resid_kernel(const ShotDev *__restrict__ shots, int nshots,
+                                                const int *__restrict__ rec_ptr, const int2 *__restrict__ rec_ent,
+                                                const float *__restrict__ resid_t, int nt, int nrec_total,
+                                                int nz, int pitch, float *au, float *aw) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nshots) return;
+    (void)nz;
+    const ShotDev sh = shots[s];
+    const size_t plane = (size_t)nt * nrec_total;
+    for (int i = 0; i < sh.nx; ++i)
+        for (int e = rec_ptr[sh.rec_row0 + i]; e < rec_ptr[sh.rec_row0 + i + 1]; ++e) {
+            const int2 en = rec_ent[e];
+            const long long o = sh.state_off + (long long)(i + 1) * pitch + en.x + COL_OFF;
+            const size_t t = (size_t)(nt - 1) * nrec_total + en.y;
+            au[o] += resid_t[t];
+            aw[o] += resid_t[2 * plane + t];
+        }
+}
+
 // Same coefficient as sponge_coef (forward_modeling.py:203-235 loop order).
 __device__ __forceinline__ float adj_sponge(const float *prof, int fw, int nz, int nx, int i, int j) {
     const int db = nz - 1 - j, dr = nx - 1 - i;

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/rtm_b200.h"
+#include "adjoint_kernels.cuh"
 #include "aux_kernels.cuh"
 #include "step_kernels.cuh"
 
@@ -520,6 +521,207 @@ int rtm_backward(rtm_plan *p, const float *obs, const float *snap_u, const float
         CUDA_TRY(cudaStreamSynchronize(s));
     }
     return RTM_OK;
+}
+
+size_t rtm_plan_state_floats(const rtm_plan *p) { return p ? p->state_floats : 0; }
+
+int rtm_plan_num_checkpoints(const rtm_plan *p, int ckpt_every) {
+    if (!p || ckpt_every <= 0) return 0;
+    const int nseg = (p->g.nt + ckpt_every - 1) / ckpt_every;
+    return nseg - 1;
+}
+
+int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, int ckpt_every, float *ckpt,
+                             int check_interval, int32_t *flags, rtm_stream_t stream) {
+    if (!p) return fail(RTM_E_ARG, "null plan");
+    if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
+    if (p->g.modes != RTM_PSV) return fail(RTM_E_ARG, "checkpointed propagation supports the P-SV mode");
+    if (ckpt_every <= 0) return fail(RTM_E_ARG, "ckpt_every must be positive");
+    if (p->nsrc_total > 0 && !wavelets) return fail(RTM_E_ARG, "null wavelets");
+    const int nt = p->g.nt;
+    const int nck = rtm_plan_num_checkpoints(p, ckpt_every);
+    if (nck > 0 && !ckpt) return fail(RTM_E_ARG, "null checkpoint buffer");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (int rc = zero_state(p, s)) return rc;
+    const size_t slot = (size_t)NADJ * p->state_floats;
+    if (nck > 0) CUDA_TRY(cudaMemsetAsync(ckpt, 0, (size_t)nck * slot * sizeof(float), s));
+    const size_t nseis = (size_t)3 * nt * p->nrec_total;
+    if (nseis) CUDA_TRY(cudaMemsetAsync(p->d_seis_t, 0, nseis * sizeof(float), s));
+    StepParams sp;
+    fill_common(p, sp);
+    sp.code_base = 1;
+    const size_t plane = (size_t)nt * p->nrec_total;
+    for (int c = 0; c < 3; ++c) {
+        sp.wav[c] = wavelets ? wavelets + (size_t)c * p->nsrc_total * nt : nullptr;
+        sp.seis[c] = p->d_seis_t + c * plane;
+    }
+    float *in[NFIELD] = {}, *out[NFIELD] = {};
+    for (int f = 0; f < NADJ; ++f) in[f] = p->d_state[0][f];
+    p->launches = 0;
+    for (int it = 0; it < nt; ++it) {
+        const bool save = (it + 1) % ckpt_every == 0 && it + 1 < nt;
+        for (int f = 0; f < NADJ; ++f) {
+            if (save) out[f] = ckpt + (size_t)((it + 1) / ckpt_every - 1) * slot + (size_t)f * p->state_floats;
+            else out[f] = (in[f] == p->d_state[0][f]) ? p->d_state[1][f] : p->d_state[0][f];
+            sp.sin[f] = in[f];
+            sp.sout[f] = out[f];
+        }
+        sp.it = it;
+        sp.check = check_interval > 0 && it % check_interval == 0;
+        CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec, p->warps, s)));
+        ++p->launches;
+        for (int f = 0; f < NADJ; ++f) in[f] = out[f];
+    }
+    if (seis && p->nrec_total) {
+        if (int rc = transpose(p->d_seis_t, seis, 3, nt, p->nrec_total, s)) return rc;
+        ++p->launches;
+    }
+    if (flags) {
+        CUDA_TRY(cudaMemcpyAsync(flags, p->d_flags, p->nshots * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    return RTM_OK;
+}
+
+int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt_every, const float *ckpt,
+                double *grad, float *grad_wavelet, rtm_stream_t stream) {
+    if (!p) return fail(RTM_E_ARG, "null plan");
+    if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
+    if (p->g.modes != RTM_PSV) return fail(RTM_E_ARG, "the adjoint supports the P-SV mode");
+    if (ckpt_every <= 0) return fail(RTM_E_ARG, "ckpt_every must be positive");
+    if (!grad) return fail(RTM_E_ARG, "null gradient output");
+    if (p->nrec_total > 0 && !resid) return fail(RTM_E_ARG, "null residual");
+    if (p->nsrc_total > 0 && !wavelets) return fail(RTM_E_ARG, "null wavelets");
+    const int nt = p->g.nt;
+    const int K = ckpt_every;
+    const int nseg = (nt + K - 1) / K;
+    if (nseg > 1 && !ckpt) return fail(RTM_E_ARG, "null checkpoint buffer");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t sf = p->state_floats;
+    const size_t slot = (size_t)NADJ * sf;
+    const size_t gfl = (size_t)p->rows_total * p->pitch;
+    // scratch: K-1 recompute slots + 1 zero state + 2 adjoint states; Kahan gradients; wavelet gradient
+    float *seg = nullptr, *gsum = nullptr, *gwt = nullptr;
+    const size_t nslots = (size_t)std::max(K - 1, 1) + 1 + 2;
+    int rc = dalloc(&seg, nslots * slot);
+    if (!rc) rc = dalloc(&gsum, (size_t)2 * NGRAD * gfl);
+    if (!rc && grad_wavelet && p->nsrc_total) rc = dalloc(&gwt, (size_t)3 * nt * p->nsrc_total);
+    auto cleanup = [&]() {
+        if (seg) cudaFree(seg);
+        if (gsum) cudaFree(gsum);
+        if (gwt) cudaFree(gwt);
+    };
+    if (rc) { cleanup(); return rc; }
+    auto body = [&]() -> int {
+        CUDA_TRY(cudaMemsetAsync(p->d_flags, 0, p->nshots * sizeof(int), s));
+        CUDA_TRY(cudaMemsetAsync(seg, 0, nslots * slot * sizeof(float), s));
+        CUDA_TRY(cudaMemsetAsync(gsum, 0, (size_t)2 * NGRAD * gfl * sizeof(float), s));
+        if (gwt) CUDA_TRY(cudaMemsetAsync(gwt, 0, (size_t)3 * nt * p->nsrc_total * sizeof(float), s));
+        if (p->nrec_total) {
+            if (int r = transpose(resid, p->d_obs_t, 3, p->nrec_total, nt, s)) return r;
+        }
+        float *zero = seg + (size_t)std::max(K - 1, 1) * slot;
+        float *adj[2] = {zero + slot, zero + 2 * slot};
+        auto fld = [&](float *base, int f) { return base + (size_t)f * sf; };
+        // a_{nt-1} = R^T g_{nt-1}
+        if (p->nrec_total) {
+            inject_last_resid_kernel<<<(p->nshots + 127) / 128, 128, 0, s>>>(
+                p->d_shots, p->nshots, p->d_rec_ptr, p->d_rec_ent, p->d_obs_t, nt, p->nrec_total,
+                p->g.nz, p->pitch, fld(adj[0], A_U), fld(adj[0], A_W));
+            CUDA_TRY(cudaGetLastError());
+        }
+        StepParams sp;
+        fill_common(p, sp);
+        sp.check = 0;
+        const size_t plane = (size_t)nt * p->nrec_total;
+        for (int c = 0; c < 3; ++c) {
+            sp.wav[c] = wavelets ? wavelets + (size_t)c * p->nsrc_total * nt : nullptr;
+            sp.seis[c] = p->d_seis_t + c * plane;  // recompute records here; not returned
+        }
+        AdjParams ap;
+        std::memset(&ap, 0, sizeof ap);
+        ap.nz = p->g.nz;
+        ap.pitch = p->pitch;
+        ap.nt = nt;
+        ap.fw = p->g.absorbing_frame;
+        ap.dt = sp.dt;
+        ap.inv_dx = sp.inv_dx;
+        ap.inv_dz = sp.inv_dz;
+        ap.src_factor = sp.src_factor;
+        ap.sponge = p->d_sponge;
+        ap.work = p->d_work;
+        ap.n_work = p->n_work;
+        ap.shots = p->d_shots;
+        for (int m = 0; m < NMAT; ++m) ap.mat[m] = p->d_mat[m];
+        ap.surface = p->has_surface ? p->d_surface : nullptr;
+        ap.src_ptr = p->d_src_ptr;
+        ap.src_ent = p->d_src_ent;
+        ap.rec_ptr = p->d_rec_ptr;
+        ap.rec_ent = p->d_rec_ent;
+        ap.nrec_total = p->nrec_total;
+        ap.nsrc_total = p->nsrc_total;
+        for (int c = 0; c < 3; ++c) {
+            ap.wav[c] = sp.wav[c];
+            ap.resid[c] = p->d_obs_t + c * plane;
+            ap.gwav[c] = gwt ? gwt + (size_t)c * nt * p->nsrc_total : nullptr;
+        }
+        for (int g = 0; g < NGRAD; ++g) {
+            ap.grad[g] = gsum + (size_t)g * gfl;
+            ap.gradc[g] = gsum + (size_t)(NGRAD + g) * gfl;
+        }
+        int cur = 0;
+        const int warps = p->warps;
+        const int blocks = (p->n_work + warps - 1) / warps;
+        p->launches = 1;
+        for (int sgi = nseg - 1; sgi >= 0; --sgi) {
+            const int start = sgi * K, end = std::min(start + K, nt);
+            float *s0 = sgi == 0 ? zero : const_cast<float *>(ckpt) + (size_t)(sgi - 1) * slot;
+            // recompute forward states start .. end-2 into seg slots 0 .. len-2
+            for (int it = start; it <= end - 2; ++it) {
+                float *src = it == start ? s0 : seg + (size_t)(it - 1 - start) * slot;
+                float *dst = seg + (size_t)(it - start) * slot;
+                for (int f = 0; f < NADJ; ++f) {
+                    sp.sin[f] = fld(src, f);
+                    sp.sout[f] = fld(dst, f);
+                }
+                sp.it = it;
+                CUDA_TRY((launch_mode<0>(sp, RTM_PSV, p->vec, warps, s)));
+                ++p->launches;
+            }
+            // reverse steps end-1 .. start
+            for (int n = end - 1; n >= start; --n) {
+                float *fs = n == start ? s0 : seg + (size_t)(n - 1 - start) * slot;
+                for (int f = 0; f < NADJ; ++f) {
+                    ap.fwd[f] = fld(fs, f);
+                    ap.ain[f] = fld(adj[cur], f);
+                    ap.aout[f] = fld(adj[1 - cur], f);
+                }
+                ap.n = n;
+                switch (p->vec) {
+                    case 1: adjoint_step_kernel<1><<<blocks, 32 * warps, 0, s>>>(ap); break;
+                    case 2: adjoint_step_kernel<2><<<blocks, 32 * warps, 0, s>>>(ap); break;
+                    default: adjoint_step_kernel<4><<<blocks, 32 * warps, 0, s>>>(ap); break;
+                }
+                CUDA_TRY(cudaGetLastError());
+                ++p->launches;
+                cur = 1 - cur;
+            }
+        }
+        const size_t n2 = (size_t)p->g.nx * p->g.nz;
+        for (int g = 0; g < NGRAD; ++g) {
+            stack_kernel<<<148 * 8, 256, 0, s>>>(ap.grad[g], ap.gradc[g], grad + g * n2, p->d_shots, p->nshots,
+                                                 p->g.nx, p->g.nz, p->pitch);
+            CUDA_TRY(cudaGetLastError());
+        }
+        if (gwt) {
+            if (int r = transpose(gwt, grad_wavelet, 3, nt, p->nsrc_total, s)) return r;
+        }
+        CUDA_TRY(cudaStreamSynchronize(s));
+        return RTM_OK;
+    };
+    rc = body();
+    cleanup();
+    return rc;
 }
 
 }  // extern "C"
