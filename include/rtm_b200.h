@@ -73,6 +73,7 @@ typedef struct {
     int vec;        /* columns per lane: 1, 2 or 4 */
     int rows;       /* rows per warp task */
     int warps;      /* warps per CTA */
+    int prefetch;   /* 1: software-pipelined row loads, 0: plain; other values = default (1) */
 } rtm_tune;
 
 /* Create a plan for nshots shots on one grid: validates geometry, builds the

@@ -56,7 +56,7 @@ int round_up(int a, int b) { return (a + b - 1) / b * b; }
 struct rtm_plan {
     rtm_grid g{};
     int nshots = 0;
-    int vec = 4, rows = 32, warps = 4;
+    int vec = 4, rows = 32, warps = 4, prefetch = 1;
     int pitch = 0;
     int nstrips = 0;
     std::vector<ShotDev> shots_h;
@@ -98,20 +98,22 @@ void plan_free(rtm_plan *p) {
     F(p->d_seis_t); F(p->d_obs_t); F(p->d_flags);
 }
 
-template <int DIR, int MODE, int VEC>
+template <int DIR, int MODE, int VEC, bool PF>
 cudaError_t launch_step(const StepParams &sp, int warps, cudaStream_t s) {
     const int threads = 32 * warps;
     const int blocks = (sp.n_work + warps - 1) / warps;
-    step_kernel<DIR, MODE, VEC><<<blocks, threads, 0, s>>>(sp);
+    step_kernel<DIR, MODE, VEC, PF><<<blocks, threads, 0, s>>>(sp);
     return cudaGetLastError();
 }
 
 template <int DIR, int MODE>
 cudaError_t launch_vec(const StepParams &sp, int vec, int warps, cudaStream_t s) {
+    const bool pf = (vec & 0x100) != 0;
+    vec &= 0xff;
     switch (vec) {
-        case 1: return launch_step<DIR, MODE, 1>(sp, warps, s);
-        case 2: return launch_step<DIR, MODE, 2>(sp, warps, s);
-        default: return launch_step<DIR, MODE, 4>(sp, warps, s);
+        case 1: return pf ? launch_step<DIR, MODE, 1, true>(sp, warps, s) : launch_step<DIR, MODE, 1, false>(sp, warps, s);
+        case 2: return pf ? launch_step<DIR, MODE, 2, true>(sp, warps, s) : launch_step<DIR, MODE, 2, false>(sp, warps, s);
+        default: return pf ? launch_step<DIR, MODE, 4, true>(sp, warps, s) : launch_step<DIR, MODE, 4, false>(sp, warps, s);
     }
 }
 
@@ -184,6 +186,7 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
         if (tune->vec == 1 || tune->vec == 2 || tune->vec == 4) p->vec = tune->vec;
         if (tune->rows > 0) p->rows = tune->rows;
         if (tune->warps > 0 && tune->warps <= 8) p->warps = tune->warps;
+        if (tune->prefetch == 0 || tune->prefetch == 1) p->prefetch = tune->prefetch;
     }
     const int W = 30 * p->vec;
     p->nstrips = (g.nz + W - 1) / W;
@@ -418,7 +421,7 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
         sp.check = check_interval > 0 && it % check_interval == 0;
         sp.snap_k = (save && it % isnap == 0 && it != 0) ? it / isnap - 1 : -1;  // fm:569-570
         if (sp.snap_k >= nsnap) sp.snap_k = -1;
-        CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec, p->warps, s)));
+        CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, s)));
         ++p->launches;
     }
     if (seis && p->nrec_total) {
@@ -488,7 +491,7 @@ int rtm_backward(rtm_plan *p, const float *obs, const float *snap_u, const float
             const int k = t / isnap - 1;
             if (k >= 0 && k < num_snaps && isnaps[k] == t) sp.snap_k = k;
         }
-        CUDA_TRY((launch_mode<1>(sp, p->g.modes, p->vec, p->warps, s)));
+        CUDA_TRY((launch_mode<1>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, s)));
         ++p->launches;
     }
     const int blocks = 148 * 8;
@@ -568,7 +571,7 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
         }
         sp.it = it;
         sp.check = check_interval > 0 && it % check_interval == 0;
-        CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec, p->warps, s)));
+        CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, s)));
         ++p->launches;
         for (int f = 0; f < NADJ; ++f) in[f] = out[f];
     }
@@ -685,7 +688,7 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
                     sp.sout[f] = fld(dst, f);
                 }
                 sp.it = it;
-                CUDA_TRY((launch_mode<0>(sp, RTM_PSV, p->vec, warps, s)));
+                CUDA_TRY((launch_mode<0>(sp, RTM_PSV, p->vec | (p->prefetch << 8), warps, s)));
                 ++p->launches;
             }
             // reverse steps end-1 .. start

@@ -137,7 +137,11 @@ __device__ __forceinline__ void kahan_add(float &sum, float &comp, float prod) {
     sum = t;
 }
 
-template <int DIR, int MODE, int VEC>
+// PF = true software-pipelines the row loop: the loads of the next row (stress,
+// velocity, inverse density, material) are issued before the current row is
+// computed, so each warp keeps about twice as many bytes in flight.  The
+// arithmetic is unchanged (bit-identical results).
+template <int DIR, int MODE, int VEC, bool PF = false>
 __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
     constexpr bool PSV = (MODE & 1) != 0;
     constexpr bool SH = (MODE & 2) != 0;
@@ -186,18 +190,54 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
             ldv<VEC>(yz, S(F_SYZ, i));
         }
     };
-    auto load_vel = [&](int i) {
+    auto load_vel_into = [&](int i, float (&a_u)[VEC], float (&a_w)[VEC], float (&a_v)[VEC],
+                             float (&b_u)[VEC], float (&b_w)[VEC], float (&b_v)[VEC]) {
         if constexpr (PSV) {
-            ldv<VEC>(vs_u, S(F_U, i));
-            ldv<VEC>(vs_w, S(F_W, i));
-            ldv<VEC>(ir_u, M(M_IRU, i));
-            ldv<VEC>(ir_w, M(M_IRW, i));
+            ldv<VEC>(a_u, S(F_U, i));
+            ldv<VEC>(a_w, S(F_W, i));
+            ldv<VEC>(b_u, M(M_IRU, i));
+            ldv<VEC>(b_w, M(M_IRW, i));
         }
         if constexpr (SH) {
-            ldv<VEC>(vs_v, S(F_V, i));
-            ldv<VEC>(ir_v, M(M_IR, i));
+            ldv<VEC>(a_v, S(F_V, i));
+            ldv<VEC>(b_v, M(M_IR, i));
         }
     };
+    auto load_vel = [&](int i) { load_vel_into(i, vs_u, vs_w, vs_v, ir_u, ir_w, ir_v); };
+    // stress-update material of the row being finished (lam, mu, mxz / myx,
+    // myz) and the surface mask
+    float lam[VEC], mu[VEC], mxz[VEC], myx[VEC], myz[VEC], sm[VEC];
+    float n_lam[VEC], n_mu[VEC], n_mxz[VEC], n_myx[VEC], n_myz[VEC], n_sm[VEC];
+    auto load_mat = [&](int r, float (&a)[VEC], float (&b)[VEC], float (&c)[VEC], float (&d)[VEC],
+                        float (&e)[VEC], float (&s)[VEC]) {
+        if constexpr (PSV) {
+            ldv<VEC>(a, M(M_LAM, r));
+            ldv<VEC>(b, M(M_MU, r));
+            ldv<VEC>(c, M(M_MXZ, r));
+        }
+        if constexpr (SH) {
+            ldv<VEC>(d, M(M_MYX, r));
+            ldv<VEC>(e, M(M_MYZ, r));
+        }
+        if (p.surface) {
+            ldv<VEC>(s, p.surface + moff + (long long)(r + 1) * P);
+        } else {
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) s[q] = 1.f;
+        }
+    };
+    auto take_mat = [&]() {
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            lam[q] = n_lam[q]; mu[q] = n_mu[q]; mxz[q] = n_mxz[q];
+            myx[q] = n_myx[q]; myz[q] = n_myz[q]; sm[q] = n_sm[q];
+        }
+    };
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+        lam[q] = mu[q] = mxz[q] = myx[q] = myz[q] = sm[q] = 0.f;
+        n_lam[q] = n_mu[q] = n_mxz[q] = n_myx[q] = n_myz[q] = n_sm[q] = 0.f;
+    }
     // Point injection into the velocities of row i (held in u_c/w_c/v_c):
     // forward sources (forward_modeling.py:421-443) or backward observed data
     // (backward_modeling.py:452-460).  Every lane that computes a column does
@@ -249,23 +289,9 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
                           const float (&va_w)[VEC], const float (&va_v)[VEC],
                           const float (&vb_u)[VEC], const float (&vb_w)[VEC],
                           const float (&vb_v)[VEC]) {
-        // va = velocities of row r, vb = the other row (r+1 forward, r-1 backward)
-        float lam[VEC], mu[VEC], mxz[VEC], myx[VEC], myz[VEC], sm[VEC];
-        if constexpr (PSV) {
-            ldv<VEC>(lam, M(M_LAM, r));
-            ldv<VEC>(mu, M(M_MU, r));
-            ldv<VEC>(mxz, M(M_MXZ, r));
-        }
-        if constexpr (SH) {
-            ldv<VEC>(myx, M(M_MYX, r));
-            ldv<VEC>(myz, M(M_MYZ, r));
-        }
-        if (p.surface) {
-            ldv<VEC>(sm, p.surface + moff + (long long)(r + 1) * P);
-        } else {
-#pragma unroll
-            for (int q = 0; q < VEC; ++q) sm[q] = 1.f;
-        }
+        // va = velocities of row r, vb = the other row (r+1 forward, r-1 backward);
+        // lam/mu/mxz/myx/myz/sm hold row r's material (loaded by the caller)
+        if constexpr (!PF) load_mat(r, lam, mu, mxz, myx, myz, sm);
         // column neighbour of row r's velocities: j+1 (forward) or j-1 (backward)
         float nu = 0.f, nw = 0.f, nv = 0.f;
         if constexpr (DIR == 0) {
@@ -402,11 +428,33 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
         // ---------------- forward: velocity row k, stress row k-1 ----------------
         load_sigma(ia - 1, sxx_p, szz_p, sxz_p, syx_p, syz_p);
         float c_prev[VEC];
+        float n_sxx[VEC], n_szz[VEC], n_sxz[VEC], n_syx[VEC], n_syz[VEC];
+        float n_vu[VEC], n_vw[VEC], n_vv[VEC], n_iu[VEC], n_iw[VEC], n_iv[VEC];
 #pragma unroll
         for (int q = 0; q < VEC; ++q) c_prev[q] = 1.f;
+        if constexpr (PF) {
+            load_sigma(ia, n_sxx, n_szz, n_sxz, n_syx, n_syz);
+            load_vel_into(ia, n_vu, n_vw, n_vv, n_iu, n_iw, n_iv);
+        }
         for (int k = ia; k <= ib; ++k) {
-            load_sigma(k, sxx_c, szz_c, sxz_c, syx_c, syz_c);
-            load_vel(k);
+            if constexpr (PF) {
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    sxx_c[q] = n_sxx[q]; szz_c[q] = n_szz[q]; sxz_c[q] = n_sxz[q];
+                    syx_c[q] = n_syx[q]; syz_c[q] = n_syz[q];
+                    vs_u[q] = n_vu[q]; vs_w[q] = n_vw[q]; vs_v[q] = n_vv[q];
+                    ir_u[q] = n_iu[q]; ir_w[q] = n_iw[q]; ir_v[q] = n_iv[q];
+                }
+                if (k > ia) take_mat();  // row k-1, prefetched one iteration ago
+                if (k < ib) {
+                    load_sigma(k + 1, n_sxx, n_szz, n_sxz, n_syx, n_syz);
+                    load_vel_into(k + 1, n_vu, n_vw, n_vv, n_iu, n_iw, n_iv);
+                    load_mat(k, n_lam, n_mu, n_mxz, n_myx, n_myz, n_sm);
+                }
+            } else {
+                load_sigma(k, sxx_c, szz_c, sxz_c, syx_c, syz_c);
+                load_vel(k);
+            }
             float szz_m = 0.f, sxz_m = 0.f, syz_m = 0.f;  // column j-1 of row k
             if constexpr (PSV) {
                 szz_m = __shfl_up_sync(FULL, szz_c[VEC - 1], 1);
@@ -452,9 +500,26 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
         // ------------- backward: velocity row k-1 (needs stress row k) -------------
         load_sigma(ia - 1, sxx_p, szz_p, sxz_p, syx_p, syz_p);
         load_vel(ia - 1);
+        float n_sxx[VEC], n_szz[VEC], n_sxz[VEC], n_syx[VEC], n_syz[VEC];
+        float n_vu[VEC], n_vw[VEC], n_vv[VEC], n_iu[VEC], n_iw[VEC], n_iv[VEC];
+        if constexpr (PF) load_sigma(ia, n_sxx, n_szz, n_sxz, n_syx, n_syz);
         for (int k = ia; k <= ib; ++k) {
             const int r = k - 1;
-            load_sigma(k, sxx_c, szz_c, sxz_c, syx_c, syz_c);
+            if constexpr (PF) {
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) {
+                    sxx_c[q] = n_sxx[q]; szz_c[q] = n_szz[q]; sxz_c[q] = n_sxz[q];
+                    syx_c[q] = n_syx[q]; syz_c[q] = n_syz[q];
+                }
+                if (k > ia) take_mat();  // row r, prefetched one iteration ago
+                if (k < ib) {
+                    load_sigma(k + 1, n_sxx, n_szz, n_sxz, n_syx, n_syz);
+                    load_vel_into(k, n_vu, n_vw, n_vv, n_iu, n_iw, n_iv);
+                    load_mat(k, n_lam, n_mu, n_mxz, n_myx, n_myz, n_sm);
+                }
+            } else {
+                load_sigma(k, sxx_c, szz_c, sxz_c, syx_c, syz_c);
+            }
             float szz_n = 0.f, sxz_n = 0.f, syz_n = 0.f;  // column j+1 of row r
             if constexpr (PSV) {
                 szz_n = __shfl_down_sync(FULL, szz_p[0], 1);
@@ -488,7 +553,17 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
             }
             inject(r);
             if (k > ia) finish_row(r, cc, u_c, w_c, v_c, u_p, w_p, v_p);
-            if (k < ib) load_vel(k);
+            if constexpr (PF) {
+                if (k < ib) {
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) {
+                        vs_u[q] = n_vu[q]; vs_w[q] = n_vw[q]; vs_v[q] = n_vv[q];
+                        ir_u[q] = n_iu[q]; ir_w[q] = n_iw[q]; ir_v[q] = n_iv[q];
+                    }
+                }
+            } else {
+                if (k < ib) load_vel(k);
+            }
 #pragma unroll
             for (int q = 0; q < VEC; ++q) {
                 sxx_p[q] = sxx_c[q]; szz_p[q] = szz_c[q]; sxz_p[q] = sxz_c[q];
