@@ -191,6 +191,7 @@ def main():
     import torch
     import torch.distributed as dist
     from taichirtm_b200.batch import BatchedRTM, survey_shots, survey_wavelets
+    from taichirtm_b200.distributed import reduce_result
     from taichirtm_b200.plan import PSV
 
     torch.cuda.set_device(local)
@@ -236,12 +237,15 @@ def main():
             ev[2].record(stream)
         return ff, fb
 
+    status = 0
     for _ in range(args.warmup):
         ff, fb = one_step()
-        assert int(ff.max()) == 0 and int(fb.max()) == 0
+        status = max(status, int(ff.max()), int(fb.max()))
     torch.cuda.synchronize()
     if world > 1:
-        dist.barrier()
+        reduce_result(torch.zeros(1, dtype=torch.float64, device=dev), status)  # all ranks agree or raise
+    elif status:
+        raise FloatingPointError(f"propagation became non-finite (code {status})")
     sampler = ClockSampler()
     sampler.start()
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
@@ -251,11 +255,12 @@ def main():
     torch.cuda.synchronize()
     t_start.record(stream)
     for k in range(args.steps):
-        one_step(evs[k])
+        ff, fb = one_step(evs[k])
+        status = max(status, int(ff.max()), int(fb.max()))
         launches += plan.launch_count()  # backward launches
         launches += nt + 1               # forward: nt step launches + seismogram transpose
     if world > 1:
-        dist.all_reduce(stack)           # cross-GPU image stack (FP64)
+        stack = reduce_result(stack, status)  # cross-GPU image stack (FP64), after a status check
     t_end.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop(os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0] or None)
@@ -297,10 +302,10 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        _, _, st = rtm.migrate(wav_h.to(dev, non_blocking=True), obs_h.to(dev, non_blocking=True),
-                               isnap=ISNAP, check_interval=100)
+        ff, fb, st = rtm.migrate(wav_h.to(dev, non_blocking=True), obs_h.to(dev, non_blocking=True),
+                                 isnap=ISNAP, check_interval=100)
         if world > 1:
-            dist.all_reduce(st)
+            st = reduce_result(st, max(int(ff.max()), int(fb.max())))
         host_img = st.cpu()
     e1.record(stream)
     torch.cuda.synchronize()
