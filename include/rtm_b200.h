@@ -74,6 +74,8 @@ typedef struct {
     int rows;       /* rows per warp task */
     int warps;      /* warps per CTA */
     int prefetch;   /* 1: software-pipelined row loads, 0: plain; other values = default (1) */
+    int graphs;     /* 1: capture each time loop as a CUDA graph on first use and replay it
+                       while its pointers and schedule stay the same; 0 = direct launches */
 } rtm_tune;
 
 /* Create a plan for nshots shots on one grid: validates geometry, builds the

@@ -15,7 +15,7 @@ CANDIDATES = [
     dict(vec=4, rows=32, warps=4, prefetch=1), dict(vec=4, rows=16, warps=4, prefetch=1),
     dict(vec=2, rows=16, warps=4, prefetch=1), dict(vec=2, rows=32, warps=4, prefetch=1),
     dict(vec=2, rows=8, warps=4, prefetch=1), dict(vec=1, rows=8, warps=4, prefetch=1),
-    dict(vec=1, rows=4, warps=2, prefetch=1), dict(vec=2, rows=4, warps=2, prefetch=1),
+    dict(vec=1, rows=4, warps=2, prefetch=1), dict(vec=2, rows=4, warps=4, prefetch=1),
     dict(vec=2, rows=16, warps=4, prefetch=0), dict(vec=4, rows=64, warps=4, prefetch=1),
 ]
 TUNE_STEPS = 24

@@ -28,7 +28,7 @@ class BatchedRTM:
     """
 
     def __init__(self, mu, lam, rho, dx, dz, fs, nt, absorbing_frame, shots: Sequence[ShotGeometry],
-                 modes=PSV, surface=None, tune="auto", device=None):
+                 modes=PSV, surface=None, tune="auto", device=None, graphs=True):
         require_cuda()
         self.device = torch.device(device if device is not None else "cuda")
         self.nx, self.nz = tuple(np.shape(mu))
@@ -40,6 +40,9 @@ class BatchedRTM:
         self._surface = None if surface is None else to_tensor(surface, torch.float32, self.device)
         if tune == "auto":
             tune = autotune.best_shape(self._make_plan, self.nz, self.shots, self.modes, self.nt)
+        # time loops replayed as CUDA graphs: repeated calls on the same buffers
+        # skip the per-step launch overhead
+        tune = dict(tune or {}, graphs=int(bool(graphs)))
         self.tune = tune
         self.plan = self._make_plan(tune, self.nt)
 

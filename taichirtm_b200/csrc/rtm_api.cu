@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstdarg>
+#include <cstdint>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -78,6 +79,16 @@ struct rtm_plan {
     int *d_flags = nullptr;
     bool model_set = false;
     long long launches = 0;
+    // CUDA-graph replay of time loops (tune.graphs): one cached executable per
+    // loop kind, keyed by every pointer and schedule value it bakes in.
+    struct GraphCache {
+        std::vector<unsigned long long> key;
+        cudaGraphExec_t exec = nullptr;
+    };
+    bool use_graphs = false;
+    cudaStream_t gstream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+    GraphCache g_fwd, g_bwd, g_ckpt;
 };
 
 namespace {
@@ -96,7 +107,55 @@ void plan_free(rtm_plan *p) {
     F(p->d_surface); F(p->d_sponge);
     for (int c = 0; c < 3; ++c) { F(p->d_img[c]); F(p->d_imgc[c]); }
     F(p->d_seis_t); F(p->d_obs_t); F(p->d_flags);
+    for (auto *gc : {&p->g_fwd, &p->g_bwd, &p->g_ckpt})
+        if (gc->exec) cudaGraphExecDestroy(gc->exec);
+    if (p->ev_in) cudaEventDestroy(p->ev_in);
+    if (p->ev_out) cudaEventDestroy(p->ev_out);
+    if (p->gstream) cudaStreamDestroy(p->gstream);
 }
+
+// Run a time loop: directly on s, or (use_graphs) as a CUDA graph captured on
+// the plan's own stream the first time this key is seen and replayed after.
+// The caller's stream and the plan stream are ordered by two events.
+template <typename Body>
+int run_loop(rtm_plan *p, rtm_plan::GraphCache &gc, const std::vector<unsigned long long> &key,
+             cudaStream_t s, Body &&body) {
+    if (!p->use_graphs) return body(s);
+    if (!p->gstream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&p->gstream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming));
+    }
+    if (!gc.exec || gc.key != key) {
+        if (gc.exec) {
+            cudaGraphExecDestroy(gc.exec);
+            gc.exec = nullptr;
+        }
+        CUDA_TRY(cudaStreamBeginCapture(p->gstream, cudaStreamCaptureModeThreadLocal));
+        const int rc = body(p->gstream);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(p->gstream, &graph);
+        if (rc || e != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc ? rc : fail(RTM_E_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+        }
+        const cudaError_t e2 = cudaGraphInstantiate(&gc.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e2 != cudaSuccess) {
+            gc.exec = nullptr;
+            return fail(RTM_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e2));
+        }
+        gc.key = key;
+    }
+    CUDA_TRY(cudaEventRecord(p->ev_in, s));
+    CUDA_TRY(cudaStreamWaitEvent(p->gstream, p->ev_in, 0));
+    CUDA_TRY(cudaGraphLaunch(gc.exec, p->gstream));
+    CUDA_TRY(cudaEventRecord(p->ev_out, p->gstream));
+    CUDA_TRY(cudaStreamWaitEvent(s, p->ev_out, 0));
+    return 0;
+}
+
+unsigned long long U(const void *ptr) { return (unsigned long long)(uintptr_t)ptr; }
 
 template <int DIR, int MODE, int VEC, bool PF>
 cudaError_t launch_step(const StepParams &sp, int warps, cudaStream_t s) {
@@ -187,6 +246,7 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
         if (tune->rows > 0) p->rows = tune->rows;
         if (tune->warps > 0 && tune->warps <= 8) p->warps = tune->warps;
         if (tune->prefetch == 0 || tune->prefetch == 1) p->prefetch = tune->prefetch;
+        p->use_graphs = tune->graphs == 1;
     }
     const int W = 30 * p->vec;
     p->nstrips = (g.nz + W - 1) / W;
@@ -412,18 +472,25 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
     sp.snap[2] = snap_w;
     sp.nsnap = nsnap;
     p->launches = 0;
-    for (int it = 0; it < nt; ++it) {
-        for (int f = 0; f < NFIELD; ++f) {
-            sp.sin[f] = p->d_state[it & 1][f];
-            sp.sout[f] = p->d_state[(it + 1) & 1][f];
+    auto loop = [&](cudaStream_t ls) -> int {
+        for (int it = 0; it < nt; ++it) {
+            for (int f = 0; f < NFIELD; ++f) {
+                sp.sin[f] = p->d_state[it & 1][f];
+                sp.sout[f] = p->d_state[(it + 1) & 1][f];
+            }
+            sp.it = it;
+            sp.check = check_interval > 0 && it % check_interval == 0;
+            sp.snap_k = (save && it % isnap == 0 && it != 0) ? it / isnap - 1 : -1;  // fm:569-570
+            if (sp.snap_k >= nsnap) sp.snap_k = -1;
+            CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, ls)));
         }
-        sp.it = it;
-        sp.check = check_interval > 0 && it % check_interval == 0;
-        sp.snap_k = (save && it % isnap == 0 && it != 0) ? it / isnap - 1 : -1;  // fm:569-570
-        if (sp.snap_k >= nsnap) sp.snap_k = -1;
-        CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, s)));
-        ++p->launches;
-    }
+        return 0;
+    };
+    const std::vector<unsigned long long> key = {U(wavelets), U(snap_u), U(snap_v), U(snap_w),
+                                                 (unsigned long long)save, (unsigned long long)isnap,
+                                                 (unsigned long long)check_interval};
+    if (int rc = run_loop(p, p->g_fwd, key, s, loop)) return rc;
+    p->launches += nt;
     if (seis && p->nrec_total) {
         if (int rc = transpose(p->d_seis_t, seis, 3, nt, p->nrec_total, s)) return rc;
         ++p->launches;
@@ -478,22 +545,34 @@ int rtm_backward(rtm_plan *p, const float *obs, const float *snap_u, const float
     }
     sp.nsnap = num_snaps;
     p->launches = 1;
+    // imaging schedule, known on the host (replaces _check_isnap_match, bm:490-496)
+    std::vector<int> snap_of(nt, -1);
     for (int it = 0; it < nt; ++it) {
-        const int t = (nt - 1) - it;  // backward_modeling.py:549
-        for (int f = 0; f < NFIELD; ++f) {
-            sp.sin[f] = p->d_state[it & 1][f];
-            sp.sout[f] = p->d_state[(it + 1) & 1][f];
-        }
-        sp.it = t;
-        sp.check = check_interval > 0 && it % check_interval == 0;
-        sp.snap_k = -1;
+        const int t = (nt - 1) - it;
         if (t > 0 && t % isnap == 0) {  // backward_modeling.py:558-564
             const int k = t / isnap - 1;
-            if (k >= 0 && k < num_snaps && isnaps[k] == t) sp.snap_k = k;
+            if (k >= 0 && k < num_snaps && isnaps[k] == t) snap_of[it] = k;
         }
-        CUDA_TRY((launch_mode<1>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, s)));
-        ++p->launches;
     }
+    auto loop = [&](cudaStream_t ls) -> int {
+        for (int it = 0; it < nt; ++it) {
+            for (int f = 0; f < NFIELD; ++f) {
+                sp.sin[f] = p->d_state[it & 1][f];
+                sp.sout[f] = p->d_state[(it + 1) & 1][f];
+            }
+            sp.it = (nt - 1) - it;  // backward_modeling.py:549
+            sp.check = check_interval > 0 && it % check_interval == 0;
+            sp.snap_k = snap_of[it];
+            CUDA_TRY((launch_mode<1>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, ls)));
+        }
+        return 0;
+    };
+    std::vector<unsigned long long> key = {U(snap_u), U(snap_v), U(snap_w), (unsigned long long)num_snaps,
+                                           (unsigned long long)isnap, (unsigned long long)check_interval};
+    for (int it = 0; it < nt; ++it)
+        if (snap_of[it] >= 0) key.push_back(((unsigned long long)it << 32) | (unsigned)snap_of[it]);
+    if (int rc = run_loop(p, p->g_bwd, key, s, loop)) return rc;
+    p->launches += nt;
     const int blocks = 148 * 8;
     if (image) {
         const size_t n = (size_t)p->g.nx * p->g.nz;

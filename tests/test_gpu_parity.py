@@ -167,6 +167,33 @@ def test_launch_shapes_agree(tune):
     assert np.array_equal(out[0][1], out[1][1])
 
 
+def test_cuda_graph_replay_matches_direct_launches():
+    """tune.graphs = 1 captures each time loop once and replays it; results
+    equal direct launches, on the capture call and on replays, and a changed
+    snapshot schedule triggers a new capture."""
+    from taichirtm_b200.plan import Plan, ShotGeometry
+    g = load_golden("fwbw_basic")
+    nx, nz, nt = int(g["nx"]), int(g["nz"]), int(g["nt"])
+    wav = torch.as_tensor(np.stack([g["wu"], g["wv"], g["ww"]]))
+    obs = torch.as_tensor(g["obs"]).float()
+    res = {}
+    for graphs in (0, 1):
+        p = Plan(nx, nz, float(g["dx"]), float(g["dz"]), nt, float(g["fs"]), int(g["fw"]), 3,
+                 [ShotGeometry(0, nx, g["src"], g["rec"])], tune=dict(graphs=graphs))
+        p.set_model(g["mu_s"], g["lam_s"], g["rho_s"])
+        out = []
+        for isnap in (3, 3, 5):
+            snaps = [p.snapshot_buffer(nt // isnap) for _ in range(3)]
+            f, seis, snaps, isn = p.forward(wav, save=True, isnap=isnap, snaps=snaps)
+            f2, img, _ = p.backward(obs, snaps, isn, len(isn), isnap)
+            out.append((seis.cpu().numpy(), img.cpu().numpy()))
+        res[graphs] = out
+        p.close()
+    for k in range(3):
+        assert np.array_equal(res[0][k][0], res[1][k][0])
+        assert np.array_equal(res[0][k][1], res[1][k][1])
+
+
 @pytest.mark.parametrize("name", ["fwbw_basic", "fwbw_topo"])
 def test_bit_exact_vs_fp32_restatement(name):
     """With FMA contraction off, each cell's FP32 arithmetic on the GPU is the
