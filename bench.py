@@ -177,16 +177,22 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--nt", type=int, default=3000)
+    ap.add_argument("--nt", type=int, default=None, help="time steps (default: the workload's)")
     ap.add_argument("--shots", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the one-shot-per-launch leg")
+    ap.add_argument("--workload", default="c3", choices=["c3", "c4", "c5"],
+                    help="c3: batched P-SV RTM (default, the headline); c4: FWI gradient, 8 shots "
+                         "1201x401; c5: large checkpointed RTM + gradient, 32 shots 4001x1601")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return reference_arm(args, rank)
+    if args.workload != "c3":
+        from taichirtm_b200 import benchmarks
+        return benchmarks.run(args)
 
     import torch
     import torch.distributed as dist
@@ -200,7 +206,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
-    survey = build_workload(args.nt)
+    survey = build_workload(args.nt or 3000)
     survey.shots = survey.shots[: args.shots]
     shots = survey_shots(survey)
     wav = torch.as_tensor(survey_wavelets(survey)).to(dev)

@@ -147,12 +147,20 @@ size_t rtm_plan_state_floats(const rtm_plan *plan);
 /* Checkpoint slots for interval ckpt_every: ceil(nt / ckpt_every) - 1. */
 int rtm_plan_num_checkpoints(const rtm_plan *plan, int ckpt_every);
 
+/* Checkpoint storage: FP32 (exact), or FP16 / BF16 with one scale per
+ * (checkpoint, field, shot): x is stored as round(x * 32752 / max|x|). */
+enum { RTM_CKPT_F32 = 0, RTM_CKPT_F16 = 1, RTM_CKPT_BF16 = 2 };
+/* Bytes of the checkpoint buffer (data and scale tables) for this interval/dtype. */
+size_t rtm_plan_checkpoint_bytes(const rtm_plan *plan, int ckpt_every, int ckpt_dtype);
+
 /* ForwardModeling.run without snapshots (forward_modeling.py:504-575) that
  * also stores the full state after every step it with (it+1) % ckpt_every == 0
- * into ckpt (rtm_plan_num_checkpoints slots of 5 * rtm_plan_state_floats
- * floats).  Storing costs no extra traffic: the step writes its output there. */
+ * (rtm_plan_num_checkpoints slots) into ckpt (rtm_plan_checkpoint_bytes).
+ * FP32 storage costs no extra traffic (the step writes its output into the
+ * slot); FP16/BF16 add an abs-max and a pack pass at checkpoint steps only. */
 int rtm_forward_checkpointed(rtm_plan *plan, const float *wavelets, float *seis, int ckpt_every,
-                             float *ckpt, int check_interval, int32_t *flags, rtm_stream_t stream);
+                             int ckpt_dtype, void *ckpt, int check_interval, int32_t *flags,
+                             rtm_stream_t stream);
 
 /* Adjoint sweep: given resid = dJ/d(seis) (3, nrec_total, nt) and the
  * checkpoints of rtm_forward_checkpointed, recompute each segment forward and
@@ -162,7 +170,19 @@ int rtm_forward_checkpointed(rtm_plan *plan, const float *wavelets, float *seis,
  * writes dJ/d(wavelets) into grad_wavelet (3, nsrc_total, nt).  Image-style
  * Kahan FP32 accumulation per shot, FP64 sum over shots.  Synchronises. */
 int rtm_adjoint(rtm_plan *plan, const float *wavelets, const float *resid, int ckpt_every,
-                const float *ckpt, double *grad, float *grad_wavelet, rtm_stream_t stream);
+                int ckpt_dtype, const void *ckpt, double *grad, float *grad_wavelet,
+                rtm_stream_t stream);
+
+/* Checkpointed RTM backward: BackwardModeling.run_calc (backward_modeling.py:
+ * 498-579) imaging against forward wavefields RECOMPUTED segment by segment
+ * from the checkpoints of rtm_forward_checkpointed instead of stored
+ * snapshots (forward_modeling.py:530-537, 569-572).  Images at the same steps
+ * as the snapshot path with interval isnap (t > 0, t % isnap == 0); with FP32
+ * checkpoints the result equals rtm_backward bit for bit.  Outputs as
+ * rtm_backward.  Synchronises. */
+int rtm_backward_checkpointed(rtm_plan *plan, const float *wavelets, const float *obs, int ckpt_every,
+                              int ckpt_dtype, const void *ckpt, int isnap, float *image, double *stack,
+                              int check_interval, int32_t *flags, rtm_stream_t stream);
 
 /* Forward propagation of ONE shot on the whole grid that allocates no device
  * memory.  No counterpart in the reference: it exists for callers that cannot

@@ -27,6 +27,7 @@ class RtmTune(ctypes.Structure):
 
 
 PSV, SH, BOTH = 1, 2, 3
+CKPT_DTYPES = {"f32": 0, "f16": 1, "bf16": 2}
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "call out of order", -4: "out of device memory",
           -5: "size above the entry point's limit"}
 
@@ -73,8 +74,10 @@ def lib():
     _sig(L, "rtm_backward", c_int, vp, vp, vp, vp, vp, I32P, c_int, c_int, vp, vp, c_int, I32P, vp)
     _sig(L, "rtm_plan_state_floats", c_size, vp)
     _sig(L, "rtm_plan_num_checkpoints", c_int, vp, c_int)
-    _sig(L, "rtm_forward_checkpointed", c_int, vp, vp, vp, c_int, vp, c_int, I32P, vp)
-    _sig(L, "rtm_adjoint", c_int, vp, vp, vp, c_int, vp, vp, vp, vp)
+    _sig(L, "rtm_plan_checkpoint_bytes", c_size, vp, c_int, c_int)
+    _sig(L, "rtm_forward_checkpointed", c_int, vp, vp, vp, c_int, c_int, vp, c_int, I32P, vp)
+    _sig(L, "rtm_adjoint", c_int, vp, vp, vp, c_int, c_int, vp, vp, vp, vp)
+    _sig(L, "rtm_backward_checkpointed", c_int, vp, vp, vp, c_int, c_int, vp, c_int, vp, vp, c_int, I32P, vp)
     for name, args in _OPTIONAL.items():
         if hasattr(L, name):
             _sig(L, name, *args)

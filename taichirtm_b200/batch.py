@@ -12,9 +12,9 @@ from typing import List, Optional, Sequence
 import numpy as np
 import torch
 
-from . import autotune
+from . import _lib, autotune
 from .fields import to_tensor
-from .plan import PSV, SH, Plan, ShotGeometry, require_cuda
+from .plan import PSV, SH, Plan, ShotGeometry, _i32p, _ptr, _stream, check, require_cuda
 
 
 class BatchedRTM:
@@ -69,18 +69,48 @@ class BatchedRTM:
         w = to_tensor(wavelets, torch.float32, self.device)
         return self.plan.forward(w, save=save, isnap=isnap, check_interval=check_interval)
 
-    def migrate(self, wavelets, observed, isnap=10, check_interval=100, stack=None):
+    def migrate(self, wavelets, observed, isnap=10, check_interval=100, stack=None, checkpoint=None):
         """Forward with snapshots, backward with imaging, FP64 stack of every
         shot's image on the global grid.  Returns (forward flags, backward
-        flags, stack (3, nx, nz) float64 on the device)."""
+        flags, stack (3, nx, nz) float64 on the device).
+
+        ``checkpoint=dict(every=K, dtype="f32"|"f16"|"bf16")`` stores the full
+        wavefield every K steps instead of snapshots and recomputes the
+        forward wavefield segment by segment during the backward pass (P-SV):
+        memory ~ (nt/K) x 5 fields instead of (nt/isnap) x 2, one extra
+        forward pass of compute; FP32 checkpoints give the same image bits."""
         w = to_tensor(wavelets, torch.float32, self.device)
         o = to_tensor(observed, torch.float32, self.device)
+        if checkpoint:
+            return self._migrate_checkpointed(w, o, isnap, check_interval, stack, checkpoint)
         ff, _, snaps, isnaps = self.plan.forward(w, save=True, isnap=isnap, check_interval=check_interval)
         if stack is None:
             stack = torch.zeros((3, self.nx, self.nz), dtype=torch.float64, device=self.device)
         fb, _, _ = self.plan.backward(o, snaps, isnaps, len(isnaps), isnap, check_interval=check_interval,
                                       image=False, stack=stack)
         del snaps
+        return ff, fb, stack
+
+    def checkpoint_bytes(self, every, dtype="f32"):
+        return int(_lib.lib().rtm_plan_checkpoint_bytes(self.plan.h, int(every), _lib.CKPT_DTYPES[dtype]))
+
+    def _migrate_checkpointed(self, w, o, isnap, check_interval, stack, checkpoint):
+        every = int(checkpoint.get("every") or max(1, round(self.nt ** 0.5)))
+        dt = _lib.CKPT_DTYPES[checkpoint.get("dtype", "f32")]
+        L = _lib.lib()
+        ck = torch.empty(max(int(L.rtm_plan_checkpoint_bytes(self.plan.h, every, dt)), 1), dtype=torch.uint8,
+                         device=self.device)
+        seis = torch.empty((3, self.plan.nrec_total, self.nt), dtype=torch.float32, device=self.device)
+        ff = np.zeros(len(self.shots), np.int32)
+        fb = np.zeros(len(self.shots), np.int32)
+        if stack is None:
+            stack = torch.zeros((3, self.nx, self.nz), dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            check(L.rtm_forward_checkpointed(self.plan.h, _ptr(w), _ptr(seis), every, dt, _ptr(ck),
+                                             int(check_interval), _i32p(ff), _stream()), "rtm_forward_checkpointed")
+            check(L.rtm_backward_checkpointed(self.plan.h, _ptr(w), _ptr(o), every, dt, _ptr(ck), int(isnap), None,
+                                              _ptr(stack), int(check_interval), _i32p(fb), _stream()),
+                  "rtm_backward_checkpointed")
         return ff, fb, stack
 
     def launch_count(self):

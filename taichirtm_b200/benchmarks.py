@@ -1,0 +1,200 @@
+"""Runners for the FWI-gradient and large checkpointed workloads
+(``python bench.py --workload c4|c5``); the default ``bench.py`` workload is
+the batched P-SV RTM.  Each prints one JSON line.
+
+c4  FWI gradient: 1201 x 401 model, dx = 5 m, dt = 0.5 ms, nt = 3000, 8
+    full-spread shots; observed data on the true model, gradient of the L2
+    misfit on vx and vz w.r.t. (vp, vs, rho) at the Gaussian-smoothed
+    (sigma 15 cells) starting model, sqrt(nt) FP32 checkpoints with recompute.
+c5  Large batched, checkpointed P-SV RTM plus gradient: 4001 x 1601, dt =
+    0.4 ms, nt = 8000, 32 shots with U{1000..2000} receivers, FP16
+    per-field-scaled checkpoints, shots processed in waves that fit HBM.
+"""
+import json
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import synthetic as S
+from .batch import BatchedRTM, survey_shots, survey_wavelets
+from .fwi import FWIProblem, l2_misfit
+from .plan import PSV
+
+
+def _ev():
+    return torch.cuda.Event(enable_timing=True)
+
+
+def _corr(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    return float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b) + 1e-300))
+
+
+def _rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-300))
+
+
+def run_c4(args):
+    nt = args.nt or 3000
+    sv = S.config4(nt=nt)
+    dev = torch.device("cuda")
+    shots = survey_shots(sv)
+    wav = torch.as_tensor(survey_wavelets(sv), device=dev)
+    true = BatchedRTM(*sv.material(), sv.dx, sv.dz, sv.fs, nt, sv.fw, shots, tune="auto", device=dev)
+    f, obs, _, _ = true.forward(wav)
+    assert int(f.max()) == 0
+    obs = obs.clone()
+    tune = true.tune
+    true.close()
+    K = max(1, round(math.sqrt(nt)))
+    prob = FWIProblem(sv.nx, sv.nz, sv.dx, sv.dz, sv.fs, nt, sv.fw, shots, wav, ckpt_every=K,
+                      tune={k: v for k, v in tune.items() if k != "graphs"}, device=dev)
+    m0 = [torch.tensor(x, dtype=torch.float64, device=dev) for x in (sv.vp_mig, sv.vs_mig, sv.rho_mig)]
+
+    def gradient():
+        m = [x.clone().requires_grad_(True) for x in m0]
+        J = l2_misfit(m[0], m[1], m[2], prob, obs)
+        J.backward()
+        return float(J), [x.grad for x in m]
+
+    for _ in range(max(1, args.warmup)):
+        J, g = gradient()
+    torch.cuda.synchronize()
+    e0, e1 = _ev(), _ev()
+    e0.record()
+    for _ in range(args.steps):
+        J, g = gradient()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    cells = sum(s.nx for s in shots) * sv.nz
+    # reference backward + imaging (zero-lag cross-correlation) with the data
+    # residual as "observed data": its image vs the exact gradient (reported)
+    rtm = BatchedRTM(*sv.material(migration=True), sv.dx, sv.dz, sv.fs, nt, sv.fw, shots,
+                     tune={k: v for k, v in tune.items() if k != "graphs"}, graphs=False, device=dev)
+    _, syn, _, _ = rtm.forward(wav)
+    resid = (syn - obs).contiguous()
+    _, _, img = rtm.migrate(wav, resid, isnap=5)
+    rtm.close()
+    img = img.cpu().numpy()
+    inner = (slice(sv.fw, sv.nx - sv.fw), slice(5, sv.nz - sv.fw))
+    image_pm = img[0] + img[2]
+    corr = {k: _corr(gk.cpu().numpy()[inner], image_pm[inner]) for k, gk in zip(("vp", "vs", "rho"), g)}
+    line = dict(metric="FWI gradient shots/s (P-SV, exact adjoint, sqrt(nt) FP32 checkpoints)",
+                value=round(len(shots) / (ms / 1000.0), 3), unit="shots/s", n_gpus=1, steps=args.steps,
+                warmup=args.warmup, ms_per_step=round(ms, 2), higher_is_better=True, dtype="f32",
+                data="synthetic", config=dict(workload="c4 FWI gradient: 8 shots, 1201x401, dx=5 m, dt=0.5 ms, "
+                                                        f"nt={nt}, L2 misfit on vx and vz, start = smoothed true model (sigma 15)",
+                                               ckpt_every=K, checkpoint_gb=round(prob.checkpoint_bytes() / 1e9, 2),
+                                               launch_shape=tune),
+                gcell_upd_per_s=round(2 * cells * nt / (ms / 1000.0) / 1e9, 2), misfit=J,
+                normalized_corr_gradient_vs_reference_rtm_image=corr,
+                note="finite-difference (FP64, 10 directions) and dot-product checks: tests/test_gpu_adjoint.py")
+    prob.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_c5(args):
+    nt = args.nt or 8000
+    sv = S.config5(nt=nt)
+    dev = torch.device("cuda")
+    wave = args.shots if args.shots != 64 else 16
+    K = max(1, round(math.sqrt(nt)))
+    isnap = 16
+    all_shots = survey_shots(sv)
+    all_wav = survey_wavelets(sv)
+    t_true = sv.material()
+    t_mig = sv.material(migration=True)
+    stack = torch.zeros((3, sv.nx, sv.nz), dtype=torch.float64, device=dev)
+    grad = None
+    t_rtm = t_grad = 0.0
+    peak_mem = 0
+    errs = {}
+    tune = None
+    for w0 in range(0, len(all_shots), wave):
+        sl = slice(w0, w0 + wave)
+        shots = all_shots[sl]
+        wav = torch.as_tensor(all_wav[:, sl], device=dev)
+        tr = BatchedRTM(*t_true, sv.dx, sv.dz, sv.fs, nt, sv.fw, shots, tune=tune or "auto", graphs=False, device=dev)
+        tune = {k: v for k, v in tr.tune.items() if k != "graphs"}
+        f, obs, _, _ = tr.forward(wav)
+        assert int(f.max()) == 0
+        obs = obs.clone()
+        tr.close()
+        rtm = BatchedRTM(*t_mig, sv.dx, sv.dz, sv.fs, nt, sv.fw, shots, tune=tune, graphs=False, device=dev)
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats()
+        a, b = _ev(), _ev()
+        a.record()
+        ff, fb, stack = rtm.migrate(wav, obs, isnap=isnap, stack=stack, checkpoint=dict(every=K, dtype="f16"))
+        b.record()
+        torch.cuda.synchronize()
+        t_rtm += a.elapsed_time(b)
+        assert int(ff.max()) == 0 and int(fb.max()) == 0
+        _, syn, _, _ = rtm.forward(wav)
+        resid = (syn - obs)
+        rtm.close()
+        prob = FWIProblem(sv.nx, sv.nz, sv.dx, sv.dz, sv.fs, nt, sv.fw, shots, wav, ckpt_every=K,
+                          ckpt_dtype="f16", tune=tune, device=dev)
+        lam, mu, rho = (torch.as_tensor(x, device=dev) for x in (t_mig[1], t_mig[0], t_mig[2]))
+        a.record()
+        d, ck, fl = prob.forward(lam, mu, rho)
+        g, _ = prob.adjoint(resid, ck)
+        b.record()
+        torch.cuda.synchronize()
+        t_grad += a.elapsed_time(b)
+        grad = g if grad is None else grad + g
+        del ck
+        prob.close()
+        peak_mem = max(peak_mem, torch.cuda.max_memory_allocated())
+        if w0 == 0:
+            # error of FP16 checkpoints against FP32 ones on a 4-shot subset
+            sub = shots[:4]
+            ws = wav[:, :4].contiguous()
+            nrec = sum(len(s.rec) for s in sub)
+            ob = obs[:, :nrec].contiguous()
+            rs = resid[:, :nrec].contiguous()
+            r2 = BatchedRTM(*t_mig, sv.dx, sv.dz, sv.fs, nt, sv.fw, sub, tune=tune, graphs=False, device=dev)
+            i16 = r2.migrate(ws, ob, isnap=isnap, checkpoint=dict(every=K, dtype="f16"))[2].cpu().numpy()
+            i32 = r2.migrate(ws, ob, isnap=isnap, checkpoint=dict(every=K, dtype="f32"))[2].cpu().numpy()
+            r2.close()
+            errs["image_f16_vs_f32_ckpt_rel_l2"] = _rel(i16[[0, 2]], i32[[0, 2]])
+            gg = {}
+            for dt in ("f16", "f32"):
+                pr = FWIProblem(sv.nx, sv.nz, sv.dx, sv.dz, sv.fs, nt, sv.fw, sub, ws, ckpt_every=K, ckpt_dtype=dt,
+                                tune=tune, device=dev)
+                d2, c2, _ = pr.forward(lam, mu, rho)
+                gg[dt] = pr.adjoint(rs, c2)[0].cpu().numpy()
+                del c2
+                pr.close()
+            errs["gradient_f16_vs_f32_ckpt_rel_l2"] = _rel(gg["f16"], gg["f32"])
+    cells = sum(s.nx for s in all_shots) * sv.nz
+    n = len(all_shots)
+    line = dict(metric="large checkpointed P-SV RTM + FWI gradient shots/s", value=round(n / ((t_rtm + t_grad) / 1000), 4),
+                unit="shots/s", n_gpus=1, steps=1, warmup=0, ms_per_step=round(t_rtm + t_grad, 1),
+                higher_is_better=True, dtype="f32 stencils, f16 checkpoints", data="synthetic",
+                config=dict(workload=f"c5: {n} shots, 4001x1601, dx=5 m, dt=0.4 ms, nt={nt}, U{{1000..2000}} receivers, "
+                                     f"waves of {wave} shots, FP16 per-field-scaled checkpoints every {K} steps, "
+                                     f"isnap={isnap}, Kahan images/gradients, FP64 cross-shot sums",
+                            launch_shape=tune),
+                rtm_shots_per_s=round(n / (t_rtm / 1000), 4), gradient_shots_per_s=round(n / (t_grad / 1000), 4),
+                rtm_gcell_upd_per_s=round(2 * cells * nt / (t_rtm / 1000) / 1e9, 2),
+                peak_device_memory_gb=round(peak_mem / 1e9, 1), errors=errs,
+                stack_finite=bool(torch.isfinite(stack).all()), grad_finite=bool(torch.isfinite(grad).all()),
+                note="FP32-stencil error against FP64 runs is measured by the parity tests; here the FP16 "
+                     "checkpoints are compared with FP32 checkpoints on the same GPU path")
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run(args):
+    torch.cuda.set_device(int(__import__("os").environ.get("LOCAL_RANK", "0")))
+    if args.workload == "c4":
+        return run_c4(args)
+    return run_c5(args)

@@ -13,6 +13,7 @@
 
 #include "../../include/rtm_b200.h"
 #include "adjoint_kernels.cuh"
+#include "checkpoint_kernels.cuh"
 #include "aux_kernels.cuh"
 #include "step_kernels.cuh"
 
@@ -613,20 +614,102 @@ int rtm_plan_num_checkpoints(const rtm_plan *p, int ckpt_every) {
     return nseg - 1;
 }
 
-int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, int ckpt_every, float *ckpt,
-                             int check_interval, int32_t *flags, rtm_stream_t stream) {
+static size_t ckpt_elem(int dtype) { return dtype == RTM_CKPT_F32 ? 4 : 2; }
+static size_t ckpt_slot_bytes(const rtm_plan *p, int dtype) {
+    return ((size_t)NADJ * p->state_floats * ckpt_elem(dtype) + 255) & ~size_t(255);
+}
+static size_t ckpt_amax_bytes(const rtm_plan *p) { return ((size_t)NADJ * p->nshots * 4 + 255) & ~size_t(255); }
+
+size_t rtm_plan_checkpoint_bytes(const rtm_plan *p, int ckpt_every, int ckpt_dtype) {
+    const int n = rtm_plan_num_checkpoints(p, ckpt_every);
+    if (n <= 0 || ckpt_dtype < RTM_CKPT_F32 || ckpt_dtype > RTM_CKPT_BF16) return 0;
+    const size_t per = ckpt_slot_bytes(p, ckpt_dtype) + (ckpt_dtype == RTM_CKPT_F32 ? 0 : ckpt_amax_bytes(p));
+    return (size_t)n * per;
+}
+
+namespace {
+
+// Checkpoint slot c: data, then (compressed dtypes) its [5][nshots] amax table.
+unsigned char *ckpt_slot(const rtm_plan *p, void *ckpt, int dtype, int c) {
+    const size_t per = ckpt_slot_bytes(p, dtype) + (dtype == RTM_CKPT_F32 ? 0 : ckpt_amax_bytes(p));
+    return static_cast<unsigned char *>(ckpt) + (size_t)c * per;
+}
+
+// Store the 5 FP32 fields `src` into compressed slot c (absmax, then pack).
+int ckpt_store(rtm_plan *p, void *ckpt, int dtype, int c, float *const *src, cudaStream_t s) {
+    unsigned char *slot = ckpt_slot(p, ckpt, dtype, c);
+    CkptParams cp{};
+    for (int f = 0; f < NADJ; ++f) cp.src[f] = src[f];
+    cp.half = slot;
+    cp.amax = reinterpret_cast<unsigned int *>(slot + ckpt_slot_bytes(p, dtype));
+    cp.shots = p->d_shots;
+    cp.nshots = p->nshots;
+    cp.pitch = p->pitch;
+    cp.sf = p->state_floats;
+    CUDA_TRY(cudaMemsetAsync(cp.amax, 0, (size_t)NADJ * p->nshots * 4, s));
+    dim3 grid(64, p->nshots, NADJ);
+    ckpt_absmax_kernel<<<grid, 256, 0, s>>>(cp);
+    CUDA_TRY(cudaGetLastError());
+    if (dtype == RTM_CKPT_F16) ckpt_pack_kernel<__half><<<grid, 256, 0, s>>>(cp);
+    else ckpt_pack_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>(cp);
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// Restore compressed slot c into the 5 FP32 fields `dst`.
+int ckpt_load(rtm_plan *p, const void *ckpt, int dtype, int c, float *const *dst, cudaStream_t s) {
+    unsigned char *slot = ckpt_slot(p, const_cast<void *>(ckpt), dtype, c);
+    CkptParams cp{};
+    for (int f = 0; f < NADJ; ++f) cp.dst[f] = dst[f];
+    cp.half = slot;
+    cp.amax = reinterpret_cast<unsigned int *>(slot + ckpt_slot_bytes(p, dtype));
+    cp.shots = p->d_shots;
+    cp.nshots = p->nshots;
+    cp.pitch = p->pitch;
+    cp.sf = p->state_floats;
+    dim3 grid(64, p->nshots, NADJ);
+    if (dtype == RTM_CKPT_F16) ckpt_unpack_kernel<__half><<<grid, 256, 0, s>>>(cp);
+    else ckpt_unpack_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>(cp);
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// Where segment sgi's start state (after step sgi*K - 1) lives: the zero
+// state for sgi = 0, the FP32 slot itself, or `stage` after unpacking.
+int segment_start(rtm_plan *p, const void *ckpt, int dtype, int sgi, float *zero, float *stage,
+                  float **out, cudaStream_t s) {
+    if (sgi == 0) {
+        *out = zero;
+        return 0;
+    }
+    if (dtype == RTM_CKPT_F32) {
+        *out = reinterpret_cast<float *>(ckpt_slot(p, const_cast<void *>(ckpt), dtype, sgi - 1));
+        return 0;
+    }
+    float *dst[NADJ];
+    for (int f = 0; f < NADJ; ++f) dst[f] = stage + (size_t)f * p->state_floats;
+    if (int rc = ckpt_load(p, ckpt, dtype, sgi - 1, dst, s)) return rc;
+    *out = stage;
+    return 0;
+}
+
+}  // namespace
+
+int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, int ckpt_every, int ckpt_dtype,
+                             void *ckpt, int check_interval, int32_t *flags, rtm_stream_t stream) {
     if (!p) return fail(RTM_E_ARG, "null plan");
     if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
     if (p->g.modes != RTM_PSV) return fail(RTM_E_ARG, "checkpointed propagation supports the P-SV mode");
     if (ckpt_every <= 0) return fail(RTM_E_ARG, "ckpt_every must be positive");
+    if (ckpt_dtype < RTM_CKPT_F32 || ckpt_dtype > RTM_CKPT_BF16) return fail(RTM_E_ARG, "bad ckpt_dtype");
     if (p->nsrc_total > 0 && !wavelets) return fail(RTM_E_ARG, "null wavelets");
     const int nt = p->g.nt;
     const int nck = rtm_plan_num_checkpoints(p, ckpt_every);
     if (nck > 0 && !ckpt) return fail(RTM_E_ARG, "null checkpoint buffer");
     cudaStream_t s = (cudaStream_t)stream;
     if (int rc = zero_state(p, s)) return rc;
-    const size_t slot = (size_t)NADJ * p->state_floats;
-    if (nck > 0) CUDA_TRY(cudaMemsetAsync(ckpt, 0, (size_t)nck * slot * sizeof(float), s));
+    if (nck > 0 && ckpt_dtype == RTM_CKPT_F32)
+        CUDA_TRY(cudaMemsetAsync(ckpt, 0, rtm_plan_checkpoint_bytes(p, ckpt_every, ckpt_dtype), s));
     const size_t nseis = (size_t)3 * nt * p->nrec_total;
     if (nseis) CUDA_TRY(cudaMemsetAsync(p->d_seis_t, 0, nseis * sizeof(float), s));
     StepParams sp;
@@ -642,9 +725,12 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
     p->launches = 0;
     for (int it = 0; it < nt; ++it) {
         const bool save = (it + 1) % ckpt_every == 0 && it + 1 < nt;
+        const int c = (it + 1) / ckpt_every - 1;
         for (int f = 0; f < NADJ; ++f) {
-            if (save) out[f] = ckpt + (size_t)((it + 1) / ckpt_every - 1) * slot + (size_t)f * p->state_floats;
-            else out[f] = (in[f] == p->d_state[0][f]) ? p->d_state[1][f] : p->d_state[0][f];
+            if (save && ckpt_dtype == RTM_CKPT_F32)  // the step writes its output into the slot
+                out[f] = reinterpret_cast<float *>(ckpt_slot(p, ckpt, ckpt_dtype, c)) + (size_t)f * p->state_floats;
+            else
+                out[f] = (in[f] == p->d_state[0][f]) ? p->d_state[1][f] : p->d_state[0][f];
             sp.sin[f] = in[f];
             sp.sout[f] = out[f];
         }
@@ -652,6 +738,10 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
         sp.check = check_interval > 0 && it % check_interval == 0;
         CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, s)));
         ++p->launches;
+        if (save && ckpt_dtype != RTM_CKPT_F32) {
+            if (int rc = ckpt_store(p, ckpt, ckpt_dtype, c, out, s)) return rc;
+            p->launches += 2;
+        }
         for (int f = 0; f < NADJ; ++f) in[f] = out[f];
     }
     if (seis && p->nrec_total) {
@@ -665,12 +755,13 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
     return RTM_OK;
 }
 
-int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt_every, const float *ckpt,
-                double *grad, float *grad_wavelet, rtm_stream_t stream) {
+int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt_every, int ckpt_dtype,
+                const void *ckpt, double *grad, float *grad_wavelet, rtm_stream_t stream) {
     if (!p) return fail(RTM_E_ARG, "null plan");
     if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
     if (p->g.modes != RTM_PSV) return fail(RTM_E_ARG, "the adjoint supports the P-SV mode");
     if (ckpt_every <= 0) return fail(RTM_E_ARG, "ckpt_every must be positive");
+    if (ckpt_dtype < RTM_CKPT_F32 || ckpt_dtype > RTM_CKPT_BF16) return fail(RTM_E_ARG, "bad ckpt_dtype");
     if (!grad) return fail(RTM_E_ARG, "null gradient output");
     if (p->nrec_total > 0 && !resid) return fail(RTM_E_ARG, "null residual");
     if (p->nsrc_total > 0 && !wavelets) return fail(RTM_E_ARG, "null wavelets");
@@ -682,9 +773,11 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
     const size_t sf = p->state_floats;
     const size_t slot = (size_t)NADJ * sf;
     const size_t gfl = (size_t)p->rows_total * p->pitch;
-    // scratch: K-1 recompute slots + 1 zero state + 2 adjoint states; Kahan gradients; wavelet gradient
+    // scratch: K-1 recompute slots, zero state, 2 adjoint states, unpack stage;
+    // Kahan gradients; wavelet gradient
     float *seg = nullptr, *gsum = nullptr, *gwt = nullptr;
-    const size_t nslots = (size_t)std::max(K - 1, 1) + 1 + 2;
+    const size_t nrec_slots = (size_t)std::max(K - 1, 1);
+    const size_t nslots = nrec_slots + 1 + 2 + (ckpt_dtype == RTM_CKPT_F32 ? 0 : 1);
     int rc = dalloc(&seg, nslots * slot);
     if (!rc) rc = dalloc(&gsum, (size_t)2 * NGRAD * gfl);
     if (!rc && grad_wavelet && p->nsrc_total) rc = dalloc(&gwt, (size_t)3 * nt * p->nsrc_total);
@@ -693,7 +786,10 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
         if (gsum) cudaFree(gsum);
         if (gwt) cudaFree(gwt);
     };
-    if (rc) { cleanup(); return rc; }
+    if (rc) {
+        cleanup();
+        return rc;
+    }
     auto body = [&]() -> int {
         CUDA_TRY(cudaMemsetAsync(p->d_flags, 0, p->nshots * sizeof(int), s));
         CUDA_TRY(cudaMemsetAsync(seg, 0, nslots * slot * sizeof(float), s));
@@ -702,8 +798,9 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
         if (p->nrec_total) {
             if (int r = transpose(resid, p->d_obs_t, 3, p->nrec_total, nt, s)) return r;
         }
-        float *zero = seg + (size_t)std::max(K - 1, 1) * slot;
+        float *zero = seg + nrec_slots * slot;
         float *adj[2] = {zero + slot, zero + 2 * slot};
+        float *stage = zero + 3 * slot;
         auto fld = [&](float *base, int f) { return base + (size_t)f * sf; };
         // a_{nt-1} = R^T g_{nt-1}
         if (p->nrec_total) {
@@ -757,7 +854,8 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
         p->launches = 1;
         for (int sgi = nseg - 1; sgi >= 0; --sgi) {
             const int start = sgi * K, end = std::min(start + K, nt);
-            float *s0 = sgi == 0 ? zero : const_cast<float *>(ckpt) + (size_t)(sgi - 1) * slot;
+            float *s0 = nullptr;
+            if (int r = segment_start(p, ckpt, ckpt_dtype, sgi, zero, stage, &s0, s)) return r;
             // recompute forward states start .. end-2 into seg slots 0 .. len-2
             for (int it = start; it <= end - 2; ++it) {
                 float *src = it == start ? s0 : seg + (size_t)(it - 1 - start) * slot;
@@ -803,6 +901,136 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
     };
     rc = body();
     cleanup();
+    return rc;
+}
+
+int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *obs, int ckpt_every,
+                              int ckpt_dtype, const void *ckpt, int isnap, float *image, double *stack,
+                              int check_interval, int32_t *flags, rtm_stream_t stream) {
+    if (!p) return fail(RTM_E_ARG, "null plan");
+    if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
+    if (p->g.modes != RTM_PSV) return fail(RTM_E_ARG, "checkpointed RTM supports the P-SV mode");
+    if (ckpt_every <= 0 || isnap <= 0) return fail(RTM_E_ARG, "ckpt_every and isnap must be positive");
+    if (ckpt_dtype < RTM_CKPT_F32 || ckpt_dtype > RTM_CKPT_BF16) return fail(RTM_E_ARG, "bad ckpt_dtype");
+    if (p->nrec_total > 0 && !obs) return fail(RTM_E_ARG, "null observed data");
+    if (p->nsrc_total > 0 && !wavelets) return fail(RTM_E_ARG, "null wavelets");
+    if (image && p->nshots != 1) return fail(RTM_E_ARG, "image output needs a single-shot plan; use stack");
+    const int nt = p->g.nt;
+    const int K = ckpt_every;
+    const int nseg = (nt + K - 1) / K;
+    if (nseg > 1 && !ckpt) return fail(RTM_E_ARG, "null checkpoint buffer");
+    const int num_snaps = nt / isnap;  // the snapshot slots the reference would allocate (fm:531)
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t sf = p->state_floats;
+    const size_t slot = (size_t)NADJ * sf;
+    const int seg_snaps = K / isnap + 1;
+    const size_t snap_comp = (size_t)seg_snaps * p->rows_total * p->pitch;
+    // scratch: recompute ping-pong (2 states), zero state, unpack stage, segment snapshots (u, w)
+    float *buf = nullptr;
+    const size_t nbuf = 4 * slot + 2 * snap_comp;
+    if (int rc = dalloc(&buf, nbuf)) return rc;
+    auto body = [&]() -> int {
+        if (int rc = zero_state(p, s)) return rc;
+        CUDA_TRY(cudaMemsetAsync(buf, 0, nbuf * sizeof(float), s));
+        const size_t img_floats = (size_t)p->rows_total * p->pitch;
+        for (int c = 0; c < 3; ++c)
+            if (p->d_img[c]) {
+                CUDA_TRY(cudaMemsetAsync(p->d_img[c], 0, img_floats * sizeof(float), s));
+                CUDA_TRY(cudaMemsetAsync(p->d_imgc[c], 0, img_floats * sizeof(float), s));
+            }
+        if (p->nrec_total) {
+            if (int r = transpose(obs, p->d_obs_t, 3, p->nrec_total, nt, s)) return r;
+        }
+        float *rec[2] = {buf, buf + slot};
+        float *zero = buf + 2 * slot, *stage = buf + 3 * slot;
+        float *snapu = buf + 4 * slot, *snapw = snapu + snap_comp;
+        const size_t plane = (size_t)nt * p->nrec_total;
+        StepParams fp;  // forward recompute
+        fill_common(p, fp);
+        fp.check = 0;
+        fp.nsnap = seg_snaps;
+        fp.snap[0] = snapu;
+        fp.snap[2] = snapw;
+        for (int c = 0; c < 3; ++c) {
+            fp.wav[c] = wavelets ? wavelets + (size_t)c * p->nsrc_total * nt : nullptr;
+            fp.seis[c] = p->d_seis_t + c * plane;  // not returned
+        }
+        StepParams bp;  // backward with imaging
+        fill_common(p, bp);
+        bp.code_base = 4;
+        bp.nsnap = seg_snaps;
+        bp.snap[0] = snapu;
+        bp.snap[2] = snapw;
+        for (int c = 0; c < 3; ++c) {
+            bp.obs[c] = p->d_obs_t + c * plane;
+            bp.img[c] = p->d_img[c];
+            bp.imgc[c] = p->d_imgc[c];
+        }
+        // imaging at t > 0, t % isnap == 0 with a snapshot slot t/isnap - 1 < nt/isnap
+        // that the forward fills (t <= nt-1): backward_modeling.py:556-564, fm:569-572
+        auto images_at = [&](int t) { return t > 0 && t % isnap == 0 && t / isnap - 1 < num_snaps && t <= nt - 1; };
+        p->launches = 1;
+        for (int sgi = nseg - 1; sgi >= 0; --sgi) {
+            const int start = sgi * K, end = std::min(start + K, nt);
+            float *s0 = nullptr;
+            if (int r = segment_start(p, ckpt, ckpt_dtype, sgi, zero, stage, &s0, s)) return r;
+            // recompute forward steps start .. end-1, keeping u, w at imaging steps
+            const int first = ((start + isnap - 1) / isnap) * isnap;  // first multiple of isnap >= start
+            for (int it = start; it < end; ++it) {
+                float *src = it == start ? s0 : rec[(it - 1 - start) & 1];
+                float *dst = rec[(it - start) & 1];
+                for (int f = 0; f < NADJ; ++f) {
+                    fp.sin[f] = src + (size_t)f * sf;
+                    fp.sout[f] = dst + (size_t)f * sf;
+                }
+                fp.it = it;
+                fp.snap_k = images_at(it) ? (it - first) / isnap : -1;
+                CUDA_TRY((launch_mode<0>(fp, RTM_PSV, p->vec | (p->prefetch << 8), p->warps, s)));
+                ++p->launches;
+            }
+            // backward iterations whose reversed time t falls in [start, end)
+            for (int t = end - 1; t >= start; --t) {
+                const int it = (nt - 1) - t;
+                for (int f = 0; f < NFIELD; ++f) {
+                    bp.sin[f] = p->d_state[it & 1][f];
+                    bp.sout[f] = p->d_state[(it + 1) & 1][f];
+                }
+                bp.it = t;
+                bp.check = check_interval > 0 && it % check_interval == 0;
+                bp.snap_k = images_at(t) ? (t - first) / isnap : -1;
+                CUDA_TRY((launch_mode<1>(bp, RTM_PSV, p->vec | (p->prefetch << 8), p->warps, s)));
+                ++p->launches;
+            }
+        }
+        const int blocks = 148 * 8;
+        if (image) {
+            const size_t n = (size_t)p->g.nx * p->g.nz;
+            for (int c = 0; c < 3; ++c) {
+                float *dst = image + c * n;
+                if (p->d_img[c]) {
+                    image_out_kernel<<<blocks, 256, 0, s>>>(p->d_img[c], p->d_imgc[c], dst, 0, p->shots_h[0].nx,
+                                                            p->g.nz, p->pitch);
+                    CUDA_TRY(cudaGetLastError());
+                } else {
+                    CUDA_TRY(cudaMemsetAsync(dst, 0, n * sizeof(float), s));
+                }
+            }
+        }
+        if (stack) {
+            const size_t n = (size_t)p->g.nx * p->g.nz;
+            for (int c = 0; c < 3; ++c)
+                if (p->d_img[c]) {
+                    stack_kernel<<<blocks, 256, 0, s>>>(p->d_img[c], p->d_imgc[c], stack + c * n, p->d_shots,
+                                                        p->nshots, p->g.nx, p->g.nz, p->pitch);
+                    CUDA_TRY(cudaGetLastError());
+                }
+        }
+        if (flags) CUDA_TRY(cudaMemcpyAsync(flags, p->d_flags, p->nshots * sizeof(int), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        return RTM_OK;
+    };
+    const int rc = body();
+    cudaFree(buf);
     return rc;
 }
 

@@ -26,33 +26,33 @@ class FWIProblem:
     LOCAL source/receiver indices), wavelets (3, nsrc_total, nt)."""
 
     def __init__(self, nx, nz, dx, dz, fs, nt, absorbing_frame, shots, wavelets, ckpt_every=None,
-                 surface=None, tune=None, device=None):
+                 surface=None, tune=None, device=None, ckpt_dtype="f32"):
         self.device = torch.device(device if device is not None else "cuda")
         self.nx, self.nz, self.nt = int(nx), int(nz), int(nt)
         self.plan = Plan(nx, nz, dx, dz, nt, fs, absorbing_frame, PSV, list(shots), tune=tune,
                          device=self.device)
         self.wavelets = to_tensor(wavelets, torch.float32, self.device)
         self.ckpt_every = int(ckpt_every or max(1, round(math.sqrt(nt))))
+        self.ckpt_dtype = _lib.CKPT_DTYPES[ckpt_dtype]
         self.surface = None if surface is None else to_tensor(surface, torch.float32, self.device)
         L = _lib.lib()
         self.n_ckpt = int(L.rtm_plan_num_checkpoints(self.plan.h, self.ckpt_every))
         self.state_floats = int(L.rtm_plan_state_floats(self.plan.h))
 
     def checkpoint_bytes(self):
-        return self.n_ckpt * 5 * self.state_floats * 4
+        return int(_lib.lib().rtm_plan_checkpoint_bytes(self.plan.h, self.ckpt_every, self.ckpt_dtype))
 
     def forward(self, lam, mu, rho):
         """Set the model, run the checkpointed forward.  Returns (seis (3,
         nrec_total, nt), checkpoint buffer, flags)."""
         self.plan.set_model(mu, lam, rho, self.surface)
-        ck = torch.empty(max(self.n_ckpt * 5 * self.state_floats, 1), dtype=torch.float32,
-                         device=self.device)
+        ck = torch.empty(max(self.checkpoint_bytes(), 1), dtype=torch.uint8, device=self.device)
         seis = torch.empty((3, self.plan.nrec_total, self.nt), dtype=torch.float32, device=self.device)
         flags = np.zeros(len(self.plan.shots), np.int32)
         with torch.cuda.device(self.device):
             check(_lib.lib().rtm_forward_checkpointed(self.plan.h, _ptr(self.wavelets), _ptr(seis),
-                                                      self.ckpt_every, _ptr(ck), 100, _i32p(flags),
-                                                      _stream()), "rtm_forward_checkpointed")
+                                                      self.ckpt_every, self.ckpt_dtype, _ptr(ck), 100,
+                                                      _i32p(flags), _stream()), "rtm_forward_checkpointed")
         return seis, ck, flags
 
     def adjoint(self, resid, ck, want_wavelet_grad=False):
@@ -63,7 +63,8 @@ class FWIProblem:
         gw = (torch.zeros_like(self.wavelets) if want_wavelet_grad and self.plan.nsrc_total else None)
         with torch.cuda.device(self.device):
             check(_lib.lib().rtm_adjoint(self.plan.h, _ptr(self.wavelets), _ptr(r), self.ckpt_every,
-                                         _ptr(ck), _ptr(grad), _ptr(gw), _stream()), "rtm_adjoint")
+                                         self.ckpt_dtype, _ptr(ck), _ptr(grad), _ptr(gw), _stream()),
+                  "rtm_adjoint")
         return grad, gw
 
     def close(self):

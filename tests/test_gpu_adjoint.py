@@ -188,3 +188,67 @@ def test_batched_gradient_is_sum_of_shot_gradients():
         one.close()
     both.close()
     assert rel_l2(grad_both.cpu().numpy(), total.cpu().numpy()) < 1e-12
+
+
+def _windowed_case(nt=200, seed=9):
+    from taichirtm_b200.plan import ShotGeometry
+    rng = np.random.default_rng(seed)
+    nx, nz, fw = 220, 60, 12
+    vp = np.clip(2000 + 600 * _smooth(rng.standard_normal((nx, nz)), 5) / 0.2, 1600, 2900)
+    lam, mu, rho = (x.astype(np.float32) for x in _lame(vp, vp / 1.8, 310 * vp ** 0.25))
+    t = np.arange(nt) / 2000.0
+    a = (np.pi * 40.0 * (t - 0.025)) ** 2
+    w = ((1 - 2 * a) * np.exp(-a)).astype(np.float32)
+    shots = []
+    for x0, n, s in [(0, 90, 40), (50, 110, 60), (130, 90, 45)]:
+        rec = np.stack([np.arange(fw, n - fw, 2), np.ones(len(range(fw, n - fw, 2)), int)], 1)
+        shots.append(ShotGeometry(x0, n, [[s, 2]], rec))
+    wav = np.zeros((3, len(shots), nt), np.float32)
+    wav[2] = w
+    wav[0] = 0.2 * w
+    return dict(nx=nx, nz=nz, nt=nt, fw=fw, lam=lam, mu=mu, rho=rho, shots=shots, wav=wav)
+
+
+def test_checkpointed_rtm_equals_snapshot_rtm_and_compressed_error():
+    """FP32 checkpoints + recompute give the snapshot path's image bit for bit;
+    FP16 / BF16 per-field-scaled checkpoints stay close (errors printed)."""
+    from taichirtm_b200.batch import BatchedRTM
+    C = _windowed_case()
+    kw = dict(tune=dict(vec=2, rows=16, warps=4), graphs=False)
+    true = BatchedRTM(C["mu"], C["lam"], 1.02 * C["rho"], 5.0, 5.0, 2000.0, C["nt"], C["fw"], C["shots"], **kw)
+    _, obs, _, _ = true.forward(C["wav"])
+    true.close()
+    rtm = BatchedRTM(C["mu"], C["lam"], C["rho"], 5.0, 5.0, 2000.0, C["nt"], C["fw"], C["shots"], **kw)
+    ff, fb, ref = rtm.migrate(C["wav"], obs, isnap=4)
+    ref = ref.cpu().numpy()
+    for every in (13, 200):
+        _, _, st = rtm.migrate(C["wav"], obs, isnap=4, checkpoint=dict(every=every, dtype="f32"))
+        assert np.array_equal(st.cpu().numpy(), ref), every
+    errs = {}
+    for dt in ("f16", "bf16"):
+        _, _, st = rtm.migrate(C["wav"], obs, isnap=4, checkpoint=dict(every=13, dtype=dt))
+        errs[dt] = rel_l2(st.cpu().numpy()[[0, 2]], ref[[0, 2]])
+    print("compressed-checkpoint image rel-L2:", errs)
+    assert errs["f16"] < 5e-3 and errs["bf16"] < 5e-2, errs
+    rtm.close()
+
+
+def test_compressed_checkpoint_gradient_error():
+    from taichirtm_b200.fwi import FWIProblem
+    P = _problem(nt=240)
+    lam, mu, rho = (torch.as_tensor(x, dtype=torch.float32) for x in _lame(P["vp"], P["vs"], P["rho"]))
+    rng = np.random.default_rng(11)
+    out = {}
+    for dt in ("f32", "f16", "bf16"):
+        prob = _fwi(P, ckpt=16)
+        prob = FWIProblem(P["nx"], P["nz"], P["dx"], P["dz"], P["fs"], P["nt"], P["fw"],
+                          prob.plan.shots, P["wav"], ckpt_every=16, ckpt_dtype=dt)
+        d, ck, _ = prob.forward(lam, mu, rho)
+        g = torch.as_tensor(np.random.default_rng(11).standard_normal(tuple(d.shape)).astype(np.float32))
+        grad, _ = prob.adjoint(g, ck)
+        out[dt] = grad.cpu().numpy()
+        prob.close()
+    e16 = rel_l2(out["f16"], out["f32"])
+    eb16 = rel_l2(out["bf16"], out["f32"])
+    print("compressed-checkpoint gradient rel-L2: f16 %.2e bf16 %.2e" % (e16, eb16))
+    assert e16 < 1e-2 and eb16 < 1e-1
