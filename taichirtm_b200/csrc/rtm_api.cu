@@ -158,22 +158,31 @@ int run_loop(rtm_plan *p, rtm_plan::GraphCache &gc, const std::vector<unsigned l
 
 unsigned long long U(const void *ptr) { return (unsigned long long)(uintptr_t)ptr; }
 
-template <int DIR, int MODE, int VEC, bool PF>
+template <int DIR, int MODE, int VEC, int PFM>
 cudaError_t launch_step(const StepParams &sp, int warps, cudaStream_t s) {
     const int threads = 32 * warps;
     const int blocks = (sp.n_work + warps - 1) / warps;
-    step_kernel<DIR, MODE, VEC, PF><<<blocks, threads, 0, s>>>(sp);
+    step_kernel<DIR, MODE, VEC, PFM><<<blocks, threads, 0, s>>>(sp);
     return cudaGetLastError();
 }
 
+template <int DIR, int MODE, int VEC>
+cudaError_t launch_pf(const StepParams &sp, int pfm, int warps, cudaStream_t s) {
+    switch (pfm) {
+        case 0: return launch_step<DIR, MODE, VEC, 0>(sp, warps, s);
+        case 1: return launch_step<DIR, MODE, VEC, 1>(sp, warps, s);
+        default: return launch_step<DIR, MODE, VEC, 2>(sp, warps, s);
+    }
+}
+
+// vec: columns per lane in bits 0-7, prefetch mode (0/1/2) in bits 8-9
 template <int DIR, int MODE>
 cudaError_t launch_vec(const StepParams &sp, int vec, int warps, cudaStream_t s) {
-    const bool pf = (vec & 0x100) != 0;
-    vec &= 0xff;
-    switch (vec) {
-        case 1: return pf ? launch_step<DIR, MODE, 1, true>(sp, warps, s) : launch_step<DIR, MODE, 1, false>(sp, warps, s);
-        case 2: return pf ? launch_step<DIR, MODE, 2, true>(sp, warps, s) : launch_step<DIR, MODE, 2, false>(sp, warps, s);
-        default: return pf ? launch_step<DIR, MODE, 4, true>(sp, warps, s) : launch_step<DIR, MODE, 4, false>(sp, warps, s);
+    const int pfm = (vec >> 8) & 3;
+    switch (vec & 0xff) {
+        case 1: return launch_pf<DIR, MODE, 1>(sp, pfm, warps, s);
+        case 2: return launch_pf<DIR, MODE, 2>(sp, pfm, warps, s);
+        default: return launch_pf<DIR, MODE, 4>(sp, pfm, warps, s);
     }
 }
 
@@ -246,7 +255,7 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
         if (tune->vec == 1 || tune->vec == 2 || tune->vec == 4) p->vec = tune->vec;
         if (tune->rows > 0) p->rows = tune->rows;
         if (tune->warps > 0 && tune->warps <= 8) p->warps = tune->warps;
-        if (tune->prefetch == 0 || tune->prefetch == 1) p->prefetch = tune->prefetch;
+        if (tune->prefetch >= 0 && tune->prefetch <= 2) p->prefetch = tune->prefetch;
         p->use_graphs = tune->graphs == 1;
     }
     const int W = 30 * p->vec;

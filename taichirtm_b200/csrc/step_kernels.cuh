@@ -110,6 +110,47 @@ __device__ __forceinline__ void stv(float *__restrict__ p, const float (&v)[VEC]
     }
 }
 
+// L2 cache policies: wavefield state is streamed once per step (evict first),
+// the shared material is re-read by every overlapping shot (evict last).
+__device__ __forceinline__ unsigned long long l2_policy_evict_first() {
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ unsigned long long l2_policy_evict_last() {
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+// Read-only vector load with an L2 cache policy.
+template <int VEC>
+__device__ __forceinline__ void ldv_pol(float (&v)[VEC], const float *__restrict__ p, unsigned long long pol) {
+    if constexpr (VEC == 4) {
+        asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+            : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
+            : "l"(p), "l"(pol));
+    } else if constexpr (VEC == 2) {
+        asm("ld.global.nc.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;" : "=f"(v[0]), "=f"(v[1]) : "l"(p), "l"(pol));
+    } else {
+        asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v[0]) : "l"(p), "l"(pol));
+    }
+}
+
+// Vector store with an L2 cache policy.
+template <int VEC>
+__device__ __forceinline__ void stv_pol(float *p, const float (&v)[VEC], unsigned long long pol) {
+    if constexpr (VEC == 4) {
+        asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;"
+                     :: "l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "l"(pol) : "memory");
+    } else if constexpr (VEC == 2) {
+        asm volatile("st.global.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;"
+                     :: "l"(p), "f"(v[0]), "f"(v[1]), "l"(pol) : "memory");
+    } else {
+        asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" :: "l"(p), "f"(v[0]), "l"(pol) : "memory");
+    }
+}
+
 // forward_modeling.py:203-235: 1 everywhere, then left, right, bottom strips,
 // later strips overwriting earlier ones.
 __device__ __forceinline__ float sponge_coef(const StepParams &p, int nx, int i, int j) {
@@ -141,8 +182,26 @@ __device__ __forceinline__ void kahan_add(float &sum, float &comp, float prod) {
 // velocity, inverse density, material) are issued before the current row is
 // computed, so each warp keeps about twice as many bytes in flight.  The
 // arithmetic is unchanged (bit-identical results).
-template <int DIR, int MODE, int VEC, bool PF = false>
+// PFM: 0 plain, 1 prefetch, 2 prefetch + L2 cache policies (state evict-first,
+// material evict-last).  None of them changes a result bit.
+template <int DIR, int MODE, int VEC, int PFM = 0>
 __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
+    constexpr bool PF = PFM >= 1;
+    constexpr bool HINT = PFM >= 2;
+    unsigned long long pol_s = 0, pol_m = 0;
+    if constexpr (HINT) {
+        pol_s = l2_policy_evict_first();
+        pol_m = l2_policy_evict_last();
+    }
+    auto LS = [&](float (&v)[VEC], const float *ptr) {
+        if constexpr (HINT) ldv_pol<VEC>(v, ptr, pol_s); else ldv<VEC>(v, ptr);
+    };
+    auto LM = [&](float (&v)[VEC], const float *ptr) {
+        if constexpr (HINT) ldv_pol<VEC>(v, ptr, pol_m); else ldv<VEC>(v, ptr);
+    };
+    auto SS = [&](float *ptr, const float (&v)[VEC]) {
+        if constexpr (HINT) stv_pol<VEC>(ptr, v, pol_s); else stv<VEC>(ptr, v);
+    };
     constexpr bool PSV = (MODE & 1) != 0;
     constexpr bool SH = (MODE & 2) != 0;
     constexpr int W = 30 * VEC;
@@ -181,26 +240,26 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
     auto load_sigma = [&](int i, float (&xx)[VEC], float (&zz)[VEC], float (&xz)[VEC],
                           float (&yx)[VEC], float (&yz)[VEC]) {
         if constexpr (PSV) {
-            ldv<VEC>(xx, S(F_SXX, i));
-            ldv<VEC>(zz, S(F_SZZ, i));
-            ldv<VEC>(xz, S(F_SXZ, i));
+            LS(xx, S(F_SXX, i));
+            LS(zz, S(F_SZZ, i));
+            LS(xz, S(F_SXZ, i));
         }
         if constexpr (SH) {
-            ldv<VEC>(yx, S(F_SYX, i));
-            ldv<VEC>(yz, S(F_SYZ, i));
+            LS(yx, S(F_SYX, i));
+            LS(yz, S(F_SYZ, i));
         }
     };
     auto load_vel_into = [&](int i, float (&a_u)[VEC], float (&a_w)[VEC], float (&a_v)[VEC],
                              float (&b_u)[VEC], float (&b_w)[VEC], float (&b_v)[VEC]) {
         if constexpr (PSV) {
-            ldv<VEC>(a_u, S(F_U, i));
-            ldv<VEC>(a_w, S(F_W, i));
-            ldv<VEC>(b_u, M(M_IRU, i));
-            ldv<VEC>(b_w, M(M_IRW, i));
+            LS(a_u, S(F_U, i));
+            LS(a_w, S(F_W, i));
+            LM(b_u, M(M_IRU, i));
+            LM(b_w, M(M_IRW, i));
         }
         if constexpr (SH) {
-            ldv<VEC>(a_v, S(F_V, i));
-            ldv<VEC>(b_v, M(M_IR, i));
+            LS(a_v, S(F_V, i));
+            LM(b_v, M(M_IR, i));
         }
     };
     auto load_vel = [&](int i) { load_vel_into(i, vs_u, vs_w, vs_v, ir_u, ir_w, ir_v); };
@@ -211,13 +270,13 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
     auto load_mat = [&](int r, float (&a)[VEC], float (&b)[VEC], float (&c)[VEC], float (&d)[VEC],
                         float (&e)[VEC], float (&s)[VEC]) {
         if constexpr (PSV) {
-            ldv<VEC>(a, M(M_LAM, r));
-            ldv<VEC>(b, M(M_MU, r));
-            ldv<VEC>(c, M(M_MXZ, r));
+            LM(a, M(M_LAM, r));
+            LM(b, M(M_MU, r));
+            LM(c, M(M_MXZ, r));
         }
         if constexpr (SH) {
-            ldv<VEC>(d, M(M_MYX, r));
-            ldv<VEC>(e, M(M_MYZ, r));
+            LM(d, M(M_MYX, r));
+            LM(e, M(M_MYZ, r));
         }
         if (p.surface) {
             ldv<VEC>(s, p.surface + moff + (long long)(r + 1) * P);
@@ -360,16 +419,16 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
         if (!owner) return;
         const long long so = soff + (long long)(r + 1) * P;
         if constexpr (PSV) {
-            stv<VEC>(p.sout[F_SXX] + so, o_sxx);
-            stv<VEC>(p.sout[F_SZZ] + so, o_szz);
-            stv<VEC>(p.sout[F_SXZ] + so, o_sxz);
-            stv<VEC>(p.sout[F_U] + so, o_u);
-            stv<VEC>(p.sout[F_W] + so, o_w);
+            SS(p.sout[F_SXX] + so, o_sxx);
+            SS(p.sout[F_SZZ] + so, o_szz);
+            SS(p.sout[F_SXZ] + so, o_sxz);
+            SS(p.sout[F_U] + so, o_u);
+            SS(p.sout[F_W] + so, o_w);
         }
         if constexpr (SH) {
-            stv<VEC>(p.sout[F_SYX] + so, o_syx);
-            stv<VEC>(p.sout[F_SYZ] + so, o_syz);
-            stv<VEC>(p.sout[F_V] + so, o_v);
+            SS(p.sout[F_SYX] + so, o_syx);
+            SS(p.sout[F_SYZ] + so, o_syz);
+            SS(p.sout[F_V] + so, o_v);
         }
         if constexpr (DIR == 0) {
             // _record_seismogram_kernel (forward_modeling.py:445-453)
