@@ -73,7 +73,8 @@ typedef struct {
     int vec;        /* columns per lane: 1, 2 or 4 */
     int rows;       /* rows per warp task */
     int warps;      /* warps per CTA */
-    int prefetch;   /* 1: software-pipelined row loads; 2: that plus L2 cache policies (state
+    int prefetch;   /* 1: software-pipelined row loads; 3: cp.async pipeline, rows 3 ahead in a
+                       per-warp shared-memory ring; 2: row loads plus L2 cache policies (state
                        evict-first, material evict-last); 0: plain; other values = default (1) */
     int graphs;     /* 1: capture each time loop as a CUDA graph on first use and replay it
                        while its pointers and schedule stay the same; 0 = direct launches */

@@ -52,8 +52,9 @@ def lib():
     global _lib
     if _lib is not None:
         return _lib
-    path = _build.LIB
-    if not os.path.exists(path) or _build._stale():
+    override = os.environ.get("TAICHIRTM_B200_LIB")  # a separately built librtm_b200.so
+    path = override or _build.LIB
+    if not override and (not os.path.exists(path) or _build._stale()):
         try:
             path = _build.build()
         except Exception as e:  # no nvcc: fail loudly, there is no CPU path

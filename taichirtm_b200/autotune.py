@@ -12,6 +12,8 @@ import os
 import torch
 
 CANDIDATES = [
+    dict(vec=4, rows=16, warps=1, prefetch=3), dict(vec=4, rows=16, warps=2, prefetch=3),
+    dict(vec=4, rows=16, warps=2, prefetch=1),
     dict(vec=4, rows=32, warps=4, prefetch=1), dict(vec=4, rows=16, warps=4, prefetch=1),
     dict(vec=2, rows=16, warps=4, prefetch=1), dict(vec=2, rows=32, warps=4, prefetch=1),
     dict(vec=2, rows=8, warps=4, prefetch=1), dict(vec=1, rows=8, warps=4, prefetch=1),

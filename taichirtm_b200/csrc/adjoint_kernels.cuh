@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
     const int4 wk = p.work[task];
     const ShotDev sh = p.shots[wk.x];
     const int nx = sh.nx, nz = p.nz, P = p.pitch;
-    const int c0 = wk.y * W - VEC + VEC * lane;
+    const int c0 = (wk.y & 0xFFFFF) * W - VEC + VEC * lane;  // bits 20+ are step-kernel hints
     const bool owner = lane >= 1 && lane <= 30;
     const int ia = wk.z, ib = wk.w;
     const long long soff = sh.state_off + (long long)(c0 + COL_OFF);

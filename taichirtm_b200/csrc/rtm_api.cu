@@ -162,7 +162,21 @@ template <int DIR, int MODE, int VEC, int PFM>
 cudaError_t launch_step(const StepParams &sp, int warps, cudaStream_t s) {
     const int threads = 32 * warps;
     const int blocks = (sp.n_work + warps - 1) / warps;
-    step_kernel<DIR, MODE, VEC, PFM><<<blocks, threads, 0, s>>>(sp);
+    size_t smem = 0;
+    if constexpr (PFM == 3) {
+        constexpr size_t kMaxSmem = 227 * 1024;  // per-block opt-in limit
+        smem = (size_t)warps * async_smem_per_warp<MODE, VEC>();
+        if (smem > kMaxSmem) return cudaErrorInvalidConfiguration;
+        static bool attr_set = false;  // per instantiation; raises the 48 KB default
+        if (!attr_set) {
+            const size_t want = std::min<size_t>(8 * async_smem_per_warp<MODE, VEC>(), kMaxSmem);
+            cudaError_t e = cudaFuncSetAttribute(step_kernel<DIR, MODE, VEC, PFM>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
+            if (e != cudaSuccess) return e;
+            attr_set = true;
+        }
+    }
+    step_kernel<DIR, MODE, VEC, PFM><<<blocks, threads, smem, s>>>(sp);
     return cudaGetLastError();
 }
 
@@ -171,7 +185,8 @@ cudaError_t launch_pf(const StepParams &sp, int pfm, int warps, cudaStream_t s) 
     switch (pfm) {
         case 0: return launch_step<DIR, MODE, VEC, 0>(sp, warps, s);
         case 1: return launch_step<DIR, MODE, VEC, 1>(sp, warps, s);
-        default: return launch_step<DIR, MODE, VEC, 2>(sp, warps, s);
+        case 2: return launch_step<DIR, MODE, VEC, 2>(sp, warps, s);
+        default: return launch_step<DIR, MODE, VEC, 3>(sp, warps, s);
     }
 }
 
@@ -255,7 +270,7 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
         if (tune->vec == 1 || tune->vec == 2 || tune->vec == 4) p->vec = tune->vec;
         if (tune->rows > 0) p->rows = tune->rows;
         if (tune->warps > 0 && tune->warps <= 8) p->warps = tune->warps;
-        if (tune->prefetch >= 0 && tune->prefetch <= 2) p->prefetch = tune->prefetch;
+        if (tune->prefetch >= 0 && tune->prefetch <= 3) p->prefetch = tune->prefetch;
         p->use_graphs = tune->graphs == 1;
     }
     const int W = 30 * p->vec;
@@ -318,9 +333,24 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
         p->shots_h.push_back(d);
         state_rows += sh.nx + 2;
         p->rows_total += sh.nx;
+        // Per task: bit 20 / 21 of the strip word = no source / no receiver in
+        // rows [ia-1, ib] and the lanes' columns [j0 - vec, j0 + 31 vec).
+        auto none_in = [&](const std::vector<int> &ptr, const std::vector<int2> &ent, int row0, int r0, int r1,
+                           int c_lo, int c_hi) {
+            for (int r = std::max(r0, 0); r <= std::min(r1, sh.nx - 1); ++r)
+                for (int e = ptr[row0 + r]; e < ptr[row0 + r + 1]; ++e)
+                    if (ent[e].x >= c_lo && ent[e].x < c_hi) return false;
+            return true;
+        };
         for (int ia = 0; ia < sh.nx; ia += p->rows)
-            for (int st = 0; st < p->nstrips; ++st)
-                work.push_back(make_int4(s, st, ia, std::min(ia + p->rows, sh.nx)));
+            for (int st = 0; st < p->nstrips; ++st) {
+                const int ib = std::min(ia + p->rows, sh.nx);
+                const int j0 = st * W, c_lo = j0 - p->vec, c_hi = j0 + 31 * p->vec;
+                int word = st;
+                if (none_in(src_ptr, src_ent, d.src_row0, ia - 1, ib, c_lo, c_hi)) word |= 1 << 20;
+                if (none_in(rec_ptr, rec_ent, d.rec_row0, ia - 1, ib, c_lo, c_hi)) word |= 1 << 21;
+                work.push_back(make_int4(s, word, ia, ib));
+            }
     }
     // Order tasks by global row so that concurrently running shots that
     // overlap read the same material rows while they are in L2.

@@ -151,6 +151,34 @@ __device__ __forceinline__ void stv_pol(float *p, const float (&v)[VEC], unsigne
     }
 }
 
+// Asynchronous global -> shared copies of one lane's VEC floats (cp.async,
+// completion tracked per thread by commit / wait groups: no spinning).
+template <int VEC>
+__device__ __forceinline__ void cp_async_vec(float *smem, const float *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    if constexpr (VEC == 4) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+    } else if constexpr (VEC == 2) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+    }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Rows in flight per warp in the asynchronous pipeline, and the fields one row
+// brings in (P-SV: sxx szz sxz u w + inv_rho_u inv_rho_w lam mu mxz; SH: syx
+// syz v + inv_rho myx myz).
+constexpr int ASYNC_DEPTH = 4;
+template <int MODE>
+__host__ __device__ constexpr int async_fields() { return ((MODE & 1) ? 10 : 0) + ((MODE & 2) ? 6 : 0); }
+template <int MODE, int VEC>
+__host__ __device__ constexpr size_t async_smem_per_warp() {
+    return (size_t)ASYNC_DEPTH * async_fields<MODE>() * 32 * VEC * sizeof(float);
+}
+
 // forward_modeling.py:203-235: 1 everywhere, then left, right, bottom strips,
 // later strips overwriting earlier ones.
 __device__ __forceinline__ float sponge_coef(const StepParams &p, int nx, int i, int j) {
@@ -183,11 +211,15 @@ __device__ __forceinline__ void kahan_add(float &sum, float &comp, float prod) {
 // computed, so each warp keeps about twice as many bytes in flight.  The
 // arithmetic is unchanged (bit-identical results).
 // PFM: 0 plain, 1 prefetch, 2 prefetch + L2 cache policies (state evict-first,
-// material evict-last).  None of them changes a result bit.
+// material evict-last), 3 asynchronous pipeline (every field of the row
+// ASYNC_DEPTH-1 ahead copied by cp.async into a per-warp shared-memory ring;
+// launch with async_smem_per_warp() bytes of dynamic shared memory per warp).
+// None of them changes a result bit.
 template <int DIR, int MODE, int VEC, int PFM = 0>
 __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
-    constexpr bool PF = PFM >= 1;
-    constexpr bool HINT = PFM >= 2;
+    constexpr bool PF = PFM == 1 || PFM == 2;
+    constexpr bool HINT = PFM == 2;
+    constexpr bool ASYNC = PFM == 3;
     unsigned long long pol_s = 0, pol_m = 0;
     if constexpr (HINT) {
         pol_s = l2_policy_evict_first();
@@ -212,10 +244,20 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
     if (__ldg(p.flags + wk.x) != 0) return;  // this shot already failed: stop it
     const ShotDev sh = p.shots[wk.x];
     const int nx = sh.nx, nz = p.nz, P = p.pitch;
-    const int j0 = wk.y * W;
+    // wk.y: strip in bits 0-19; bit 20 / 21 set = no source / no receiver in
+    // this task's rows and columns (the row-table lookups can be skipped)
+    const int j0 = (wk.y & 0xFFFFF) * W;
+    const bool no_src = (wk.y >> 20) & 1, no_rec = (wk.y >> 21) & 1;
     const int c0 = j0 - VEC + VEC * lane;
     const bool owner = lane >= 1 && lane <= 30;
     const int ia = wk.z, ib = wk.w;
+    // warp-uniform-per-row fast paths: a lane whose columns are all interior
+    // and at least FW above the bottom edge needs the per-cell interior and
+    // sponge logic only on rows near the left/right edges
+    const bool lane_in = c0 >= 1 && c0 + VEC - 1 <= nz - 2;
+    const bool lane_far = nz - 1 - (c0 + VEC - 1) >= p.fw;
+    auto all_in = [&](int i) { return lane_in && i >= 1 && i <= nx - 2; };
+    auto all_far = [&](int i) { return lane_far && i >= p.fw && nx - 1 - i >= p.fw; };
     const long long soff = sh.state_off + (long long)(c0 + COL_OFF);
     const long long moff = (long long)sh.x0 * P + (long long)(c0 + COL_OFF);
     const float dt = p.dt, idx = p.inv_dx, idz = p.inv_dz;
@@ -303,6 +345,7 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
     // it, halo lanes included, so halo velocities are exact.
     auto inject = [&](int i) {
         if (i < 0 || i >= nx) return;
+        if ((DIR == 0 && no_src) || (DIR == 1 && no_rec)) return;
         if constexpr (DIR == 0) {
             const int e0 = __ldg(p.src_ptr + sh.src_row0 + i), e1 = __ldg(p.src_ptr + sh.src_row0 + i + 1);
             for (int e = e0; e < e1; ++e) {
@@ -350,7 +393,7 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
                           const float (&vb_v)[VEC]) {
         // va = velocities of row r, vb = the other row (r+1 forward, r-1 backward);
         // lam/mu/mxz/myx/myz/sm hold row r's material (loaded by the caller)
-        if constexpr (!PF) load_mat(r, lam, mu, mxz, myx, myz, sm);
+        if constexpr (!PF && !ASYNC) load_mat(r, lam, mu, mxz, myx, myz, sm);
         // column neighbour of row r's velocities: j+1 (forward) or j-1 (backward)
         float nu = 0.f, nw = 0.f, nv = 0.f;
         if constexpr (DIR == 0) {
@@ -362,10 +405,11 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
         }
         float o_sxx[VEC], o_szz[VEC], o_sxz[VEC], o_syx[VEC], o_syz[VEC];
         float o_u[VEC], o_w[VEC], o_v[VEC];
+        const bool rin = all_in(r);
 #pragma unroll
         for (int q = 0; q < VEC; ++q) {
             const int j = c0 + q;
-            const bool in = interior(r, j, nx, nz);
+            const bool in = rin || interior(r, j, nx, nz);
             if constexpr (PSV) {
                 float u_x, u_z, w_x, w_z;
                 if constexpr (DIR == 0) {
@@ -432,7 +476,8 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
         }
         if constexpr (DIR == 0) {
             // _record_seismogram_kernel (forward_modeling.py:445-453)
-            const int e0 = __ldg(p.rec_ptr + sh.rec_row0 + r), e1 = __ldg(p.rec_ptr + sh.rec_row0 + r + 1);
+            const int e0 = no_rec ? 0 : __ldg(p.rec_ptr + sh.rec_row0 + r);
+            const int e1 = no_rec ? 0 : __ldg(p.rec_ptr + sh.rec_row0 + r + 1);
             for (int e = e0; e < e1; ++e) {
                 const int2 en = __ldg(p.rec_ent + e);
                 const int q = en.x - c0;
@@ -483,9 +528,79 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
         }
     };
 
+    // ---- asynchronous pipeline (PFM 3): per-warp ring of ASYNC_DEPTH rows in
+    // shared memory; each lane copies and later reads back only its own VEC
+    // columns, so the only synchronisation is the lane's own wait_group.
+    constexpr int NLF = async_fields<MODE>();
+    extern __shared__ float step_smem[];
+    float *ring = step_smem + (size_t)(threadIdx.x >> 5) * (ASYNC_DEPTH * (NLF > 0 ? NLF : 1) * 32 * VEC);
+    auto slot = [&](int row, int f) {
+        const int s = (row + ASYNC_DEPTH) % ASYNC_DEPTH;  // rows start at -1
+        return ring + ((size_t)(s * NLF + f) * 32 + lane) * VEC;
+    };
+    auto issue_row = [&](int row) {
+        if (row <= ib) {
+            if constexpr (PSV) {
+                cp_async_vec<VEC>(slot(row, 0), S(F_SXX, row));
+                cp_async_vec<VEC>(slot(row, 1), S(F_SZZ, row));
+                cp_async_vec<VEC>(slot(row, 2), S(F_SXZ, row));
+                cp_async_vec<VEC>(slot(row, 3), S(F_U, row));
+                cp_async_vec<VEC>(slot(row, 4), S(F_W, row));
+                cp_async_vec<VEC>(slot(row, 5), M(M_IRU, row));
+                cp_async_vec<VEC>(slot(row, 6), M(M_IRW, row));
+                cp_async_vec<VEC>(slot(row, 7), M(M_LAM, row));
+                cp_async_vec<VEC>(slot(row, 8), M(M_MU, row));
+                cp_async_vec<VEC>(slot(row, 9), M(M_MXZ, row));
+            }
+            if constexpr (SH) {
+                constexpr int o = PSV ? 10 : 0;
+                cp_async_vec<VEC>(slot(row, o + 0), S(F_SYX, row));
+                cp_async_vec<VEC>(slot(row, o + 1), S(F_SYZ, row));
+                cp_async_vec<VEC>(slot(row, o + 2), S(F_V, row));
+                cp_async_vec<VEC>(slot(row, o + 3), M(M_IR, row));
+                cp_async_vec<VEC>(slot(row, o + 4), M(M_MYX, row));
+                cp_async_vec<VEC>(slot(row, o + 5), M(M_MYZ, row));
+            }
+        }
+        cp_async_commit();  // one group per row, empty past ib, so the counts stay aligned
+    };
+    auto rd = [&](int row, int f, float (&v)[VEC]) {
+        const float *s = slot(row, f);
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) v[q] = s[q];
+    };
+    auto rd_sigma = [&](int row, float (&xx)[VEC], float (&zz)[VEC], float (&xz)[VEC], float (&yx)[VEC],
+                        float (&yz)[VEC]) {
+        if constexpr (PSV) { rd(row, 0, xx); rd(row, 1, zz); rd(row, 2, xz); }
+        if constexpr (SH) { constexpr int o = PSV ? 10 : 0; rd(row, o + 0, yx); rd(row, o + 1, yz); }
+    };
+    auto rd_vel = [&](int row) {
+        if constexpr (PSV) { rd(row, 3, vs_u); rd(row, 4, vs_w); rd(row, 5, ir_u); rd(row, 6, ir_w); }
+        if constexpr (SH) { constexpr int o = PSV ? 10 : 0; rd(row, o + 2, vs_v); rd(row, o + 3, ir_v); }
+    };
+    auto rd_mat = [&](int row) {
+        if constexpr (PSV) { rd(row, 7, lam); rd(row, 8, mu); rd(row, 9, mxz); }
+        if constexpr (SH) { constexpr int o = PSV ? 10 : 0; rd(row, o + 4, myx); rd(row, o + 5, myz); }
+        if (p.surface) {
+            ldv<VEC>(sm, p.surface + moff + (long long)(row + 1) * P);
+        } else {
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) sm[q] = 1.f;
+        }
+    };
+    // prologue: rows ia-1 .. ia+DEPTH-3 in flight, then row ia-1's stress in registers
+    if constexpr (ASYNC) {
+#pragma unroll
+        for (int t = 0; t < ASYNC_DEPTH - 1; ++t) issue_row(ia - 1 + t);
+        cp_async_wait<ASYNC_DEPTH - 2>();
+        rd_sigma(ia - 1, sxx_p, szz_p, sxz_p, syx_p, syz_p);
+        if constexpr (DIR == 1) rd_vel(ia - 1);
+        issue_row(ia + ASYNC_DEPTH - 2);
+    }
+
     if constexpr (DIR == 0) {
         // ---------------- forward: velocity row k, stress row k-1 ----------------
-        load_sigma(ia - 1, sxx_p, szz_p, sxz_p, syx_p, syz_p);
+        if constexpr (!ASYNC) load_sigma(ia - 1, sxx_p, szz_p, sxz_p, syx_p, syz_p);
         float c_prev[VEC];
         float n_sxx[VEC], n_szz[VEC], n_sxz[VEC], n_syx[VEC], n_syz[VEC];
         float n_vu[VEC], n_vw[VEC], n_vv[VEC], n_iu[VEC], n_iw[VEC], n_iv[VEC];
@@ -496,7 +611,13 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
             load_vel_into(ia, n_vu, n_vw, n_vv, n_iu, n_iw, n_iv);
         }
         for (int k = ia; k <= ib; ++k) {
-            if constexpr (PF) {
+            if constexpr (ASYNC) {
+                cp_async_wait<ASYNC_DEPTH - 2>();  // row k has landed
+                rd_sigma(k, sxx_c, szz_c, sxz_c, syx_c, syz_c);
+                rd_vel(k);
+                if (k > ia) rd_mat(k - 1);
+                issue_row(k + ASYNC_DEPTH - 1);   // reuses row k-1's slot, read above
+            } else if constexpr (PF) {
 #pragma unroll
                 for (int q = 0; q < VEC; ++q) {
                     sxx_c[q] = n_sxx[q]; szz_c[q] = n_szz[q]; sxz_c[q] = n_sxz[q];
@@ -520,11 +641,12 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
                 sxz_m = __shfl_up_sync(FULL, sxz_c[VEC - 1], 1);
             }
             if constexpr (SH) syz_m = __shfl_up_sync(FULL, syz_c[VEC - 1], 1);
+            const bool kin = all_in(k), kfar = all_far(k);
 #pragma unroll
             for (int q = 0; q < VEC; ++q) {
                 const int j = c0 + q;
-                const bool in = interior(k, j, nx, nz);
-                cc[q] = sponge_coef(p, nx, k, j);
+                const bool in = kin || interior(k, j, nx, nz);
+                cc[q] = kfar ? 1.0f : sponge_coef(p, nx, k, j);
                 if constexpr (PSV) {
                     const float sxz_jm = q > 0 ? sxz_c[q - 1] : sxz_m;
                     const float szz_jm = q > 0 ? szz_c[q - 1] : szz_m;
@@ -557,14 +679,24 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
         }
     } else {
         // ------------- backward: velocity row k-1 (needs stress row k) -------------
-        load_sigma(ia - 1, sxx_p, szz_p, sxz_p, syx_p, syz_p);
-        load_vel(ia - 1);
+        if constexpr (!ASYNC) {
+            load_sigma(ia - 1, sxx_p, szz_p, sxz_p, syx_p, syz_p);
+            load_vel(ia - 1);
+        }
         float n_sxx[VEC], n_szz[VEC], n_sxz[VEC], n_syx[VEC], n_syz[VEC];
         float n_vu[VEC], n_vw[VEC], n_vv[VEC], n_iu[VEC], n_iw[VEC], n_iv[VEC];
         if constexpr (PF) load_sigma(ia, n_sxx, n_szz, n_sxz, n_syx, n_syz);
         for (int k = ia; k <= ib; ++k) {
             const int r = k - 1;
-            if constexpr (PF) {
+            if constexpr (ASYNC) {
+                cp_async_wait<ASYNC_DEPTH - 2>();  // row k has landed
+                rd_sigma(k, sxx_c, szz_c, sxz_c, syx_c, syz_c);
+                if (k > ia) {
+                    rd_vel(r);  // row r's velocity inputs (row ia-1's came in the prologue)
+                    rd_mat(r);
+                }
+                issue_row(k + ASYNC_DEPTH - 1);   // reuses row r's slot, read above
+            } else if constexpr (PF) {
 #pragma unroll
                 for (int q = 0; q < VEC; ++q) {
                     sxx_c[q] = n_sxx[q]; szz_c[q] = n_szz[q]; sxz_c[q] = n_sxz[q];
@@ -585,11 +717,12 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
                 sxz_n = __shfl_down_sync(FULL, sxz_p[0], 1);
             }
             if constexpr (SH) syz_n = __shfl_down_sync(FULL, syz_p[0], 1);
+            const bool rin = all_in(r), rfar = all_far(r);
 #pragma unroll
             for (int q = 0; q < VEC; ++q) {
                 const int j = c0 + q;
-                const bool in = interior(r, j, nx, nz);
-                cc[q] = sponge_coef(p, nx, r, j);
+                const bool in = rin || interior(r, j, nx, nz);
+                cc[q] = rfar ? 1.0f : sponge_coef(p, nx, r, j);
                 if constexpr (PSV) {
                     const float sxz_jp = q < VEC - 1 ? sxz_p[q + 1] : sxz_n;
                     const float szz_jp = q < VEC - 1 ? szz_p[q + 1] : szz_n;
@@ -620,7 +753,7 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
                         ir_u[q] = n_iu[q]; ir_w[q] = n_iw[q]; ir_v[q] = n_iv[q];
                     }
                 }
-            } else {
+            } else if constexpr (!ASYNC) {
                 if (k < ib) load_vel(k);
             }
 #pragma unroll

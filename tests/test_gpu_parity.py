@@ -145,7 +145,7 @@ def test_config2_sh_vs_fp64_oracle_short():
     assert e <= SEIS_TOL, e
 
 
-@pytest.mark.parametrize("tune", [dict(vec=1, rows=7, warps=2, prefetch=0), dict(vec=2, rows=16, warps=4, prefetch=1),
+@pytest.mark.parametrize("tune", [dict(vec=1, rows=7, warps=2, prefetch=0), dict(vec=2, rows=16, warps=4, prefetch=1), dict(vec=2, rows=9, warps=3, prefetch=3), dict(vec=4, rows=16, warps=2, prefetch=3), dict(vec=1, rows=3, warps=2, prefetch=3),
                                   dict(vec=4, rows=64, warps=8, prefetch=0), dict(vec=2, rows=5, warps=1, prefetch=1)])
 def test_launch_shapes_agree(tune):
     """Every launch shape gives the same seismograms and images (bit-exact:
