@@ -171,6 +171,79 @@ def reference_arm(args, rank):
     return 0
 
 
+# ------------------------------------------------------------- plain one-shot RTM
+def plain_single_shot(args, rank):
+    """Plain single-shot RTM (forward with snapshots at the reference's
+    interval, backward with imaging) on the full model: 301 x 151 P-SV (c1) or
+    1001 x 501 SH (c2), the CPU restatement timed beside it."""
+    if rank != 0:
+        return 0
+    import torch
+    from taichirtm_b200 import autotune, synthetic as S
+    from taichirtm_b200.plan import PSV, SH, Plan, ShotGeometry
+    from oracle import c_oracle
+    cfg = S.config1() if args.workload == "c1" else S.config2()
+    modes, isnap = (PSV, 1) if args.workload == "c1" else (SH, 7)
+    sh = cfg.shots[0]
+    geo = [ShotGeometry(0, cfg.nx, sh.src, sh.rec)]
+    mk = lambda tune, nt: Plan(cfg.nx, cfg.nz, cfg.dx, cfg.dz, nt, cfg.fs, cfg.fw, modes, geo, tune=tune)  # noqa: E731
+
+    def make(tune, nt):
+        p = mk(tune, nt)
+        p.set_model(*cfg.material(migration=True))
+        return p
+    tune = dict(autotune.best_shape(make, cfg.nz, geo, modes, cfg.nt) or {}, graphs=1)
+    true = mk(tune, cfg.nt)
+    true.set_model(*cfg.material())
+    wav = torch.as_tensor(sh.wavelets).cuda()
+    _, obs, _, _ = true.forward(wav)
+    obs = obs.clone()
+    true.close()
+    p = make(tune, cfg.nt)
+    nsnap = cfg.nt // isnap
+    snaps = [p.snapshot_buffer(nsnap) if (c == 1) == (modes == SH) else None for c in range(3)]
+
+    def rtm():
+        f1, _, sn, isn = p.forward(wav, save=True, isnap=isnap, snaps=snaps)
+        f2, img, _ = p.backward(obs, sn, isn, len(isn), isnap)
+        return f1, f2, img
+    for _ in range(max(3, args.warmup)):
+        f1, f2, img = rtm()
+    assert int(f1.max()) == 0 and int(f2.max()) == 0
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        rtm()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    cells = cfg.nx * cfg.nz
+    # CPU: the reference algorithm (both modes, as the reference advances) on all host cores
+    mu, lam, rho = cfg.material(migration=True)
+    nthreads = os.cpu_count() or 1
+    n_run = min(cfg.nt, 400 if args.workload == "c1" else 100)
+    kw = dict(dx=cfg.dx, dz=cfg.dz, nt=cfg.nt, fs=cfg.fs, fw=cfg.fw, dtype=np.float32, modes=3, nthreads=nthreads)
+    t0 = time.perf_counter()
+    f = c_oracle.forward(mu, lam, rho, src=sh.src, wu=sh.wavelets[0], wv=sh.wavelets[1], ww=sh.wavelets[2],
+                         rec=sh.rec, nt_run=n_run, save=True, isnap=isnap, **kw)
+    c_oracle.backward(mu, lam, rho, rec=sh.rec, obs=np.zeros((3, len(sh.rec), cfg.nt), np.float32),
+                      snaps=f["snaps"], isnaps=f["isnaps"], num_snaps=f["num_snaps"], isnap=isnap, nt_run=n_run, **kw)
+    cpu_s = (time.perf_counter() - t0) * cfg.nt / n_run
+    line = dict(metric=METRIC, value=round(1000.0 / ms, 3), unit="shots/s", n_gpus=1, steps=args.steps,
+                warmup=args.warmup, ms_per_step=round(ms, 3), higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="f32", data="synthetic",
+                config=dict(workload=cfg.name + f": {cfg.nx}x{cfg.nz}, nt={cfg.nt}, isnap={isnap}, one shot, "
+                            "forward with snapshots + backward with imaging", launch_shape=tune),
+                gcell_upd_per_s=round(2 * cells * cfg.nt / (ms / 1000.0) / 1e9, 2),
+                us_per_step=round(ms * 1000.0 / (2 * cfg.nt), 2),
+                cpu_baseline=dict(value=round(1.0 / cpu_s, 4), unit="shots/s", cores=nthreads, kind="port",
+                                  sample=f"{n_run} of {cfg.nt} steps per phase, both P-SV and SH, FP32, scaled"))
+    print(json.dumps(line), flush=True)
+    p.close()
+    return 0
+
+
 # --------------------------------------------------------------------------- GPU
 def main():
     ap = argparse.ArgumentParser()
@@ -182,7 +255,7 @@ def main():
     ap.add_argument("--shots", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the one-shot-per-launch leg")
-    ap.add_argument("--workload", default="c3", choices=["c3", "c4", "c5"],
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c3: batched P-SV RTM (default, the headline); c4: FWI gradient, 8 shots "
                          "1201x401; c5: large checkpointed RTM + gradient, 32 shots 4001x1601")
     args = ap.parse_args()
@@ -191,6 +264,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return reference_arm(args, rank)
+    if args.workload in ("c1", "c2"):
+        return plain_single_shot(args, rank)
     if args.workload != "c3":
         from taichirtm_b200 import benchmarks
         return benchmarks.run(args)
