@@ -6,9 +6,9 @@ Workload (one "step"): 64 shots of the batched P-SV RTM configuration -- a
 anomalies), shot k at x index 55 + 30 k with U{200..800} receivers in a window
 +- a 50-cell sponge -- migrated in one pass: forward with snapshots every 16
 steps, backward with Kahan zero-lag cross-correlation, FP64 stack of all 64
-images on the global grid.  Each time step of each phase is ONE kernel launch
-covering all 64 shots.  Observed data are modelled on the true model before
-timing.
+images on the global grid.  Each kernel launch advances all 64 shots by one
+time step, or by two (temporal blocking, when the autotuner picks it).
+Observed data are modelled on the true model before timing.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -50,12 +50,14 @@ def peak_hbm():
         return PEAK_FALLBACK_GBS, "fallback"
 
 
-def ncu_traffic_per_cell():
-    """DRAM bytes per cell-update of the step kernel from the committed ncu
-    summary (profiles/step_kernel_traffic.json), or None."""
+def ncu_traffic_per_cell(tsteps=1):
+    """DRAM bytes per shot cell of ONE launch of the step kernel that runs
+    `tsteps` time steps per launch, from the committed ncu summary
+    (profiles/step_kernel_traffic.json), or None."""
     try:
         with open(os.path.join(ROOT, "profiles", "step_kernel_traffic.json")) as f:
-            return float(json.load(f)["dram_bytes_per_cell_update"])
+            k = json.load(f)["kernels"][str(int(tsteps))]
+        return float(k["dram_bytes_per_shot_cell_per_launch"])
     except Exception:
         return None
 
@@ -255,6 +257,9 @@ def main():
     ap.add_argument("--shots", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the one-shot-per-launch leg")
+    ap.add_argument("--tune", default=None,
+                    help='fixed launch shape as JSON, e.g. \'{"vec": 2, "rows": 32, "warps": 1, "tsteps": 2}\' '
+                         "(default: the autotuner's choice)")
     ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c3: batched P-SV RTM (default, the headline); c4: FWI gradient, 8 shots "
                          "1201x401; c5: large checkpointed RTM + gradient, 32 shots 4001x1601")
@@ -291,14 +296,14 @@ def main():
 
     # observed data: forward on the true model (untimed)
     true = BatchedRTM(mu_t, lam_t, rho_t, survey.dx, survey.dz, survey.fs, survey.nt, survey.fw, shots,
-                      modes=PSV, tune="auto", device=dev)
+                      modes=PSV, tune=json.loads(args.tune) if args.tune else "auto", device=dev)
     flags, obs, _, _ = true.forward(wav, save=False, check_interval=100)
     assert int(flags.max()) == 0, flags
     obs = obs.clone()
     true.close()
     del true
     rtm = BatchedRTM(mu_m, lam_m, rho_m, survey.dx, survey.dz, survey.fs, survey.nt, survey.fw, shots,
-                     modes=PSV, tune="auto", device=dev)
+                     modes=PSV, tune=json.loads(args.tune) if args.tune else "auto", device=dev)
     plan = rtm.plan
     cells = rtm.cells()
     nt = survey.nt
@@ -311,17 +316,19 @@ def main():
         if ev:
             ev[0].record(stream)
         ff, _, snaps, isnaps = plan.forward(wav, save=True, isnap=ISNAP, check_interval=100)
+        n_launch = plan.launch_count()  # step launches + seismogram transpose
         if ev:
             ev[1].record(stream)
         fb, _, _ = plan.backward(obs, snaps, isnaps, len(isnaps), ISNAP, check_interval=100, image=False,
                                  stack=stack)
+        n_launch += plan.launch_count()  # transpose + step launches + stack
         if ev:
             ev[2].record(stream)
-        return ff, fb
+        return ff, fb, n_launch
 
     status = 0
     for _ in range(args.warmup):
-        ff, fb = one_step()
+        ff, fb, _ = one_step()
         status = max(status, int(ff.max()), int(fb.max()))
     torch.cuda.synchronize()
     if world > 1:
@@ -337,10 +344,9 @@ def main():
     torch.cuda.synchronize()
     t_start.record(stream)
     for k in range(args.steps):
-        ff, fb = one_step(evs[k])
+        ff, fb, n_launch = one_step(evs[k])
         status = max(status, int(ff.max()), int(fb.max()))
-        launches += plan.launch_count()  # backward launches
-        launches += nt + 1               # forward: nt step launches + seismogram transpose
+        launches += n_launch
     if world > 1:
         stack = reduce_result(stack, status)  # cross-GPU image stack (FP64), after a status check
     t_end.record(stream)
@@ -371,21 +377,30 @@ def main():
     n_snap_writes = nsnap if nsnap * ISNAP <= nt - 1 else nsnap - 1
     alg_fwd = nt * step_bytes + n_snap_writes * SNAP_BYTES_PER_CELL * cells
     alg_bwd = nt * step_bytes + n_img * IMG_BYTES_PER_CELL * cells
-    per_launch_bytes = (alg_fwd + alg_bwd) / (2 * nt)
-    per_launch_ms = (fwd_ms + bwd_ms) / args.steps / (2 * nt)
-    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    # per time step (the unit of the byte model); a launch runs tsteps steps
+    tsteps = int(rtm.tune.get("tsteps", 1) or 1)
+    per_step_bytes = (alg_fwd + alg_bwd) / (2 * nt)
+    per_step_ms = (fwd_ms + bwd_ms) / args.steps / (2 * nt)
+    achieved = per_step_bytes / (per_step_ms * 1e-3) / 1e9
     peak, peak_kind = peak_hbm()
-    tpc = ncu_traffic_per_cell()
+    tpc = ncu_traffic_per_cell(tsteps)
     roofline = dict(bound="hbm", achieved=round(achieved, 1), peak=peak, unit="GB/s",
                     frac=round(achieved / peak, 4),
                     traffic=(round(tpc * cells) if tpc else None),
-                    kernel="step_kernel<fwd|bwd, P-SV> (one launch = one time step of all shots)",
-                    bytes_per_launch=int(per_launch_bytes), us_per_launch=round(per_launch_ms * 1e3, 2),
-                    bytes_model=("40 B per shot cell (state R+W) + 20 B per model cell under any window "
-                                 "(material read once) per step; + snapshot / imaging bytes"),
+                    kernel=(f"step2_kernel<fwd|bwd, P-SV>: one launch = {tsteps} time steps of all shots"
+                            if tsteps == 2 else "step_kernel<fwd|bwd, P-SV>: one launch = one time step of all shots"),
+                    steps_per_launch=tsteps,
+                    bytes_per_launch=int(per_step_bytes * tsteps), us_per_launch=round(per_step_ms * tsteps * 1e3, 2),
+                    bytes_model=("algorithmic bytes per time step: 40 B per shot cell (state R+W) + 20 B per "
+                                 "model cell under any window (material read once) + snapshot / imaging bytes; "
+                                 "x steps per launch. traffic = ncu DRAM bytes of one launch"),
                     achieved_if_material_per_shot=round(
-                        (per_launch_bytes + MATERIAL_BYTES_PER_CELL * (cells - union_cells)) / (per_launch_ms * 1e-3) / 1e9, 1),
+                        (per_step_bytes + MATERIAL_BYTES_PER_CELL * (cells - union_cells)) / (per_step_ms * 1e-3) / 1e9, 1),
                     peak_source=peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind)
+    if tpc:
+        dram_gbs = tpc * cells / (per_step_ms * tsteps * 1e-3) / 1e9
+        roofline["dram_achieved"] = round(dram_gbs, 1)
+        roofline["dram_frac"] = round(dram_gbs / peak, 4)
 
     # end to end through the public API: host inputs, device outputs read back
     wav_h = wav.cpu().pin_memory()
@@ -425,7 +440,7 @@ def main():
             o0 = sum(len(x.src) for x in shots[:s])
             r0 = sum(len(x.rec) for x in shots[:s])
             one = BatchedRTM(mu_m, lam_m, rho_m, survey.dx, survey.dz, survey.fs, nt, survey.fw, sub,
-                             modes=PSV, tune=dict(vec=2, rows=16, warps=4), device=dev)
+                             modes=PSV, tune=dict(vec=2, rows=16, warps=4, tsteps=tsteps), device=dev)
             w1 = wav[:, o0:o0 + ns].contiguous()
             o1 = obs[:, r0:r0 + len(sub[0].rec)].contiguous()
             one.migrate(w1, o1, isnap=ISNAP)

@@ -78,6 +78,9 @@ typedef struct {
                        evict-first, material evict-last); 0: plain; other values = default (1) */
     int graphs;     /* 1: capture each time loop as a CUDA graph on first use and replay it
                        while its pointers and schedule stay the same; 0 = direct launches */
+    int tsteps;     /* time steps per launch of rtm_forward, rtm_backward and the
+                       checkpointed entry points: 2 = temporal blocking (needs vec 2 or 4;
+                       bit-identical results), 1 or 0 = one step per launch */
 } rtm_tune;
 
 /* Create a plan for nshots shots on one grid: validates geometry, builds the

@@ -23,7 +23,7 @@ class RtmShot(ctypes.Structure):
 
 class RtmTune(ctypes.Structure):
     _fields_ = [("vec", ctypes.c_int), ("rows", ctypes.c_int), ("warps", ctypes.c_int),
-                ("prefetch", ctypes.c_int), ("graphs", ctypes.c_int)]
+                ("prefetch", ctypes.c_int), ("graphs", ctypes.c_int), ("tsteps", ctypes.c_int)]
 
 
 PSV, SH, BOTH = 1, 2, 3

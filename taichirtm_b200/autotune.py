@@ -1,7 +1,7 @@
 """Launch-shape autotuner for the fused step kernels.
 
-The shape is (vec columns per lane, rows per warp task, warps per CTA).
-Results never depend on it (every cell's arithmetic is the same; FMA
+The shape is (vec columns per lane, rows per warp task, warps per CTA, load
+pipeline, time steps per launch).  Results never depend on it (every cell's arithmetic is the same; FMA
 contraction is off), so the tuner only times: it builds a short plan for each
 candidate, times a few forward steps with CUDA events, and caches the best
 per (GPU, nz, total window rows, shots, modes) in a JSON file
@@ -12,6 +12,11 @@ import os
 import torch
 
 CANDIDATES = [
+    # two time steps per launch (temporal blocking; vec 2 or 4)
+    dict(vec=2, rows=32, warps=1, tsteps=2), dict(vec=2, rows=16, warps=2, tsteps=2),
+    dict(vec=2, rows=8, warps=2, tsteps=2), dict(vec=4, rows=32, warps=1, tsteps=2),
+    dict(vec=2, rows=4, warps=4, tsteps=2),
+    # one time step per launch
     dict(vec=4, rows=16, warps=1, prefetch=3), dict(vec=4, rows=16, warps=2, prefetch=3),
     dict(vec=4, rows=16, warps=2, prefetch=1),
     dict(vec=4, rows=32, warps=4, prefetch=1), dict(vec=4, rows=16, warps=4, prefetch=1),
@@ -52,7 +57,7 @@ def _store(cache):
 def key(nz, shots, modes):
     name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
     rows = sum(s.nx for s in shots)
-    return f"{name}|nz={nz}|rows={rows}|shots={len(shots)}|modes={modes}"
+    return f"{name}|nz={nz}|rows={rows}|shots={len(shots)}|modes={modes}|v2"
 
 
 def time_shape(make_plan, shots, tune, steps=TUNE_STEPS):

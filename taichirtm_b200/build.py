@@ -11,7 +11,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "librtm_b200.so")
 SOURCES = ["rtm_api.cu", "noalloc.cu"]
-DEPS = ["step_kernels.cuh", "aux_kernels.cuh", "adjoint_kernels.cuh", "noalloc.cu"]
+DEPS = ["step_kernels.cuh", "step2_kernels.cuh", "checkpoint_kernels.cuh", "aux_kernels.cuh", "adjoint_kernels.cuh", "noalloc.cu"]
 # -fmad=false: no FMA contraction, so every cell's FP32 arithmetic follows the
 # reference's expression order exactly and results do not depend on the launch
 # shape the autotuner picks (the kernels are HBM-bound; FLOPs are free).

@@ -15,6 +15,7 @@
 #include "adjoint_kernels.cuh"
 #include "checkpoint_kernels.cuh"
 #include "aux_kernels.cuh"
+#include "step2_kernels.cuh"
 #include "step_kernels.cuh"
 
 using namespace rtm;
@@ -59,6 +60,7 @@ struct rtm_plan {
     rtm_grid g{};
     int nshots = 0;
     int vec = 4, rows = 32, warps = 4, prefetch = 1;
+    int tsteps = 1;  // time steps per launch of the propagation loops (1 or 2)
     int pitch = 0;
     int nstrips = 0;
     std::vector<ShotDev> shots_h;
@@ -210,6 +212,41 @@ cudaError_t launch_mode(const StepParams &sp, int modes, int vec, int warps, cud
     }
 }
 
+template <int DIR, int MODE, int VEC>
+cudaError_t launch_step2(const StepParams &sp, int warps, cudaStream_t s) {
+    step2_kernel<DIR, MODE, VEC><<<(sp.n_work + warps - 1) / warps, 32 * warps, 0, s>>>(sp);
+    return cudaGetLastError();
+}
+
+// Two steps (sp.it, sp.it2) in one launch; vec is 2 or 4 (checked at plan creation).
+template <int DIR>
+cudaError_t launch_mode2(const StepParams &sp, int modes, int vec, int warps, cudaStream_t s) {
+    switch (modes) {
+        case RTM_PSV: return vec == 2 ? launch_step2<DIR, RTM_PSV, 2>(sp, warps, s) : launch_step2<DIR, RTM_PSV, 4>(sp, warps, s);
+        case RTM_SH: return vec == 2 ? launch_step2<DIR, RTM_SH, 2>(sp, warps, s) : launch_step2<DIR, RTM_SH, 4>(sp, warps, s);
+        default: return vec == 2 ? launch_step2<DIR, RTM_BOTH, 2>(sp, warps, s) : launch_step2<DIR, RTM_BOTH, 4>(sp, warps, s);
+    }
+}
+
+// The launches of a time loop over loop steps 0 .. nt-1: step `it` alone, or
+// steps it and it+1 together when the plan runs two steps per launch and
+// step `it` may be the first of a pair (pairable(it): it is not checked and
+// its state need not be stored).
+struct LoopLaunch {
+    int it;
+    bool two;
+};
+template <typename Pairable>
+std::vector<LoopLaunch> loop_schedule(int first, int end, int tsteps, Pairable &&pairable) {
+    std::vector<LoopLaunch> out;
+    for (int it = first; it < end;) {
+        const bool two = tsteps == 2 && it + 1 < end && pairable(it);
+        out.push_back({it, two});
+        it += two ? 2 : 1;
+    }
+    return out;
+}
+
 void fill_common(const rtm_plan *p, StepParams &sp) {
     std::memset(&sp, 0, sizeof sp);
     const double dt = 1.0 / p->g.fs;
@@ -272,6 +309,13 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
         if (tune->warps > 0 && tune->warps <= 8) p->warps = tune->warps;
         if (tune->prefetch >= 0 && tune->prefetch <= 3) p->prefetch = tune->prefetch;
         p->use_graphs = tune->graphs == 1;
+        if (tune->tsteps == 2) {
+            if (p->vec == 1) {
+                delete p;
+                return fail(RTM_E_ARG, "two steps per launch need vec 2 or 4");
+            }
+            p->tsteps = 2;
+        }
     }
     const int W = 30 * p->vec;
     p->nstrips = (g.nz + W - 1) / W;
@@ -334,7 +378,8 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
         state_rows += sh.nx + 2;
         p->rows_total += sh.nx;
         // Per task: bit 20 / 21 of the strip word = no source / no receiver in
-        // rows [ia-1, ib] and the lanes' columns [j0 - vec, j0 + 31 vec).
+        // rows [ia-2, ib+1] (every row a one- or two-step launch updates) and
+        // the lanes' columns [j0 - vec, j0 + 31 vec).
         auto none_in = [&](const std::vector<int> &ptr, const std::vector<int2> &ent, int row0, int r0, int r1,
                            int c_lo, int c_hi) {
             for (int r = std::max(r0, 0); r <= std::min(r1, sh.nx - 1); ++r)
@@ -347,8 +392,8 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
                 const int ib = std::min(ia + p->rows, sh.nx);
                 const int j0 = st * W, c_lo = j0 - p->vec, c_hi = j0 + 31 * p->vec;
                 int word = st;
-                if (none_in(src_ptr, src_ent, d.src_row0, ia - 1, ib, c_lo, c_hi)) word |= 1 << 20;
-                if (none_in(rec_ptr, rec_ent, d.rec_row0, ia - 1, ib, c_lo, c_hi)) word |= 1 << 21;
+                if (none_in(src_ptr, src_ent, d.src_row0, ia - 2, ib + 1, c_lo, c_hi)) word |= 1 << 20;
+                if (none_in(rec_ptr, rec_ent, d.rec_row0, ia - 2, ib + 1, c_lo, c_hi)) word |= 1 << 21;
                 work.push_back(make_int4(s, word, ia, ib));
             }
     }
@@ -512,17 +557,30 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
     sp.snap[2] = snap_w;
     sp.nsnap = nsnap;
     p->launches = 0;
+    auto check_at = [&](int it) { return check_interval > 0 && it % check_interval == 0; };
+    auto snap_at = [&](int it) {
+        const int k = (save && it % isnap == 0 && it != 0) ? it / isnap - 1 : -1;  // fm:569-570
+        return k < nsnap ? k : -1;
+    };
+    const std::vector<LoopLaunch> sched = loop_schedule(0, nt, p->tsteps, [&](int it) { return !check_at(it); });
     auto loop = [&](cudaStream_t ls) -> int {
-        for (int it = 0; it < nt; ++it) {
+        for (size_t L = 0; L < sched.size(); ++L) {
+            const int it = sched[L].it;
             for (int f = 0; f < NFIELD; ++f) {
-                sp.sin[f] = p->d_state[it & 1][f];
-                sp.sout[f] = p->d_state[(it + 1) & 1][f];
+                sp.sin[f] = p->d_state[L & 1][f];
+                sp.sout[f] = p->d_state[(L + 1) & 1][f];
             }
             sp.it = it;
-            sp.check = check_interval > 0 && it % check_interval == 0;
-            sp.snap_k = (save && it % isnap == 0 && it != 0) ? it / isnap - 1 : -1;  // fm:569-570
-            if (sp.snap_k >= nsnap) sp.snap_k = -1;
-            CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, ls)));
+            sp.snap_k = snap_at(it);
+            if (sched[L].two) {
+                sp.it2 = it + 1;
+                sp.snap_k2 = snap_at(it + 1);
+                sp.check = check_at(it + 1);
+                CUDA_TRY((launch_mode2<0>(sp, p->g.modes, p->vec, p->warps, ls)));
+            } else {
+                sp.check = check_at(it);
+                CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, ls)));
+            }
         }
         return 0;
     };
@@ -530,7 +588,7 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
                                                  (unsigned long long)save, (unsigned long long)isnap,
                                                  (unsigned long long)check_interval};
     if (int rc = run_loop(p, p->g_fwd, key, s, loop)) return rc;
-    p->launches += nt;
+    p->launches += (long long)sched.size();
     if (seis && p->nrec_total) {
         if (int rc = transpose(p->d_seis_t, seis, 3, nt, p->nrec_total, s)) return rc;
         ++p->launches;
@@ -594,16 +652,26 @@ int rtm_backward(rtm_plan *p, const float *obs, const float *snap_u, const float
             if (k >= 0 && k < num_snaps && isnaps[k] == t) snap_of[it] = k;
         }
     }
+    auto check_at = [&](int it) { return check_interval > 0 && it % check_interval == 0; };
+    const std::vector<LoopLaunch> sched = loop_schedule(0, nt, p->tsteps, [&](int it) { return !check_at(it); });
     auto loop = [&](cudaStream_t ls) -> int {
-        for (int it = 0; it < nt; ++it) {
+        for (size_t L = 0; L < sched.size(); ++L) {
+            const int it = sched[L].it;
             for (int f = 0; f < NFIELD; ++f) {
-                sp.sin[f] = p->d_state[it & 1][f];
-                sp.sout[f] = p->d_state[(it + 1) & 1][f];
+                sp.sin[f] = p->d_state[L & 1][f];
+                sp.sout[f] = p->d_state[(L + 1) & 1][f];
             }
             sp.it = (nt - 1) - it;  // backward_modeling.py:549
-            sp.check = check_interval > 0 && it % check_interval == 0;
             sp.snap_k = snap_of[it];
-            CUDA_TRY((launch_mode<1>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, ls)));
+            if (sched[L].two) {
+                sp.it2 = (nt - 1) - (it + 1);
+                sp.snap_k2 = snap_of[it + 1];
+                sp.check = check_at(it + 1);
+                CUDA_TRY((launch_mode2<1>(sp, p->g.modes, p->vec, p->warps, ls)));
+            } else {
+                sp.check = check_at(it);
+                CUDA_TRY((launch_mode<1>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, ls)));
+            }
         }
         return 0;
     };
@@ -612,7 +680,7 @@ int rtm_backward(rtm_plan *p, const float *obs, const float *snap_u, const float
     for (int it = 0; it < nt; ++it)
         if (snap_of[it] >= 0) key.push_back(((unsigned long long)it << 32) | (unsigned)snap_of[it]);
     if (int rc = run_loop(p, p->g_bwd, key, s, loop)) return rc;
-    p->launches += nt;
+    p->launches += (long long)sched.size();
     const int blocks = 148 * 8;
     if (image) {
         const size_t n = (size_t)p->g.nx * p->g.nz;
@@ -762,9 +830,14 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
     float *in[NFIELD] = {}, *out[NFIELD] = {};
     for (int f = 0; f < NADJ; ++f) in[f] = p->d_state[0][f];
     p->launches = 0;
-    for (int it = 0; it < nt; ++it) {
-        const bool save = (it + 1) % ckpt_every == 0 && it + 1 < nt;
-        const int c = (it + 1) / ckpt_every - 1;
+    auto check_at = [&](int it) { return check_interval > 0 && it % check_interval == 0; };
+    auto save_at = [&](int it) { return (it + 1) % ckpt_every == 0 && it + 1 < nt; };
+    const std::vector<LoopLaunch> sched =
+        loop_schedule(0, nt, p->tsteps, [&](int it) { return !check_at(it) && !save_at(it); });
+    for (const LoopLaunch &ln : sched) {
+        const int last = ln.two ? ln.it + 1 : ln.it;  // the step whose state the launch writes
+        const bool save = save_at(last);
+        const int c = (last + 1) / ckpt_every - 1;
         for (int f = 0; f < NADJ; ++f) {
             if (save && ckpt_dtype == RTM_CKPT_F32)  // the step writes its output into the slot
                 out[f] = reinterpret_cast<float *>(ckpt_slot(p, ckpt, ckpt_dtype, c)) + (size_t)f * p->state_floats;
@@ -773,9 +846,15 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
             sp.sin[f] = in[f];
             sp.sout[f] = out[f];
         }
-        sp.it = it;
-        sp.check = check_interval > 0 && it % check_interval == 0;
-        CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, s)));
+        sp.it = ln.it;
+        sp.check = check_at(last);
+        if (ln.two) {
+            sp.it2 = last;
+            sp.snap_k2 = -1;
+            CUDA_TRY((launch_mode2<0>(sp, p->g.modes, p->vec, p->warps, s)));
+        } else {
+            CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, s)));
+        }
         ++p->launches;
         if (save && ckpt_dtype != RTM_CKPT_F32) {
             if (int rc = ckpt_store(p, ckpt, ckpt_dtype, c, out, s)) return rc;
@@ -1008,37 +1087,58 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
         // imaging at t > 0, t % isnap == 0 with a snapshot slot t/isnap - 1 < nt/isnap
         // that the forward fills (t <= nt-1): backward_modeling.py:556-564, fm:569-572
         auto images_at = [&](int t) { return t > 0 && t % isnap == 0 && t / isnap - 1 < num_snaps && t <= nt - 1; };
+        auto check_at = [&](int it) { return check_interval > 0 && it % check_interval == 0; };
         p->launches = 1;
+        long long nb = 0;  // backward launches so far: the ping-pong parity
         for (int sgi = nseg - 1; sgi >= 0; --sgi) {
             const int start = sgi * K, end = std::min(start + K, nt);
             float *s0 = nullptr;
             if (int r = segment_start(p, ckpt, ckpt_dtype, sgi, zero, stage, &s0, s)) return r;
             // recompute forward steps start .. end-1, keeping u, w at imaging steps
             const int first = ((start + isnap - 1) / isnap) * isnap;  // first multiple of isnap >= start
-            for (int it = start; it < end; ++it) {
-                float *src = it == start ? s0 : rec[(it - 1 - start) & 1];
-                float *dst = rec[(it - start) & 1];
+            auto slot_at = [&](int t) { return images_at(t) ? (t - first) / isnap : -1; };
+            const std::vector<LoopLaunch> fsched = loop_schedule(start, end, p->tsteps, [](int) { return true; });
+            for (size_t L = 0; L < fsched.size(); ++L) {
+                const int it = fsched[L].it;
+                float *src = L == 0 ? s0 : rec[(L - 1) & 1];
+                float *dst = rec[L & 1];
                 for (int f = 0; f < NADJ; ++f) {
                     fp.sin[f] = src + (size_t)f * sf;
                     fp.sout[f] = dst + (size_t)f * sf;
                 }
                 fp.it = it;
-                fp.snap_k = images_at(it) ? (it - first) / isnap : -1;
-                CUDA_TRY((launch_mode<0>(fp, RTM_PSV, p->vec | (p->prefetch << 8), p->warps, s)));
+                fp.snap_k = slot_at(it);
+                if (fsched[L].two) {
+                    fp.it2 = it + 1;
+                    fp.snap_k2 = slot_at(it + 1);
+                    CUDA_TRY((launch_mode2<0>(fp, RTM_PSV, p->vec, p->warps, s)));
+                } else {
+                    CUDA_TRY((launch_mode<0>(fp, RTM_PSV, p->vec | (p->prefetch << 8), p->warps, s)));
+                }
                 ++p->launches;
             }
-            // backward iterations whose reversed time t falls in [start, end)
-            for (int t = end - 1; t >= start; --t) {
-                const int it = (nt - 1) - t;
+            // backward iterations it whose reversed time t = nt-1-it falls in [start, end)
+            const std::vector<LoopLaunch> bsched =
+                loop_schedule(nt - end, nt - start, p->tsteps, [&](int it) { return !check_at(it); });
+            for (const LoopLaunch &ln : bsched) {
+                const int it = ln.it, t = (nt - 1) - it;
                 for (int f = 0; f < NFIELD; ++f) {
-                    bp.sin[f] = p->d_state[it & 1][f];
-                    bp.sout[f] = p->d_state[(it + 1) & 1][f];
+                    bp.sin[f] = p->d_state[nb & 1][f];
+                    bp.sout[f] = p->d_state[(nb + 1) & 1][f];
                 }
                 bp.it = t;
-                bp.check = check_interval > 0 && it % check_interval == 0;
-                bp.snap_k = images_at(t) ? (t - first) / isnap : -1;
-                CUDA_TRY((launch_mode<1>(bp, RTM_PSV, p->vec | (p->prefetch << 8), p->warps, s)));
+                bp.snap_k = slot_at(t);
+                if (ln.two) {
+                    bp.it2 = t - 1;
+                    bp.snap_k2 = slot_at(t - 1);
+                    bp.check = check_at(it + 1);
+                    CUDA_TRY((launch_mode2<1>(bp, RTM_PSV, p->vec, p->warps, s)));
+                } else {
+                    bp.check = check_at(it);
+                    CUDA_TRY((launch_mode<1>(bp, RTM_PSV, p->vec | (p->prefetch << 8), p->warps, s)));
+                }
                 ++p->launches;
+                ++nb;
             }
         }
         const int blocks = 148 * 8;

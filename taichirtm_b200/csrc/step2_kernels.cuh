@@ -1,0 +1,535 @@
+// Two time steps per launch (temporal blocking) of the fused elastic step.
+//
+// step2_kernel advances every shot by steps A (time p.it) and B (time p.it2)
+// in one pass over the wavefield: the state is read once (before A) and
+// written once (after B), the material once, so a launch costs the HBM
+// traffic of one single step for two steps of work.  Every cell's
+// arithmetic is the single-step kernel's, operation by operation, so the
+// result is bit-identical to two launches of step_kernel.
+//
+// Dependencies.  One step reaches one row and one column in each direction:
+// forward, the velocity of row i reads the stress of rows i-1, i and the
+// stress of row i reads the new velocity of rows i, i+1; backward the other
+// way round (backward_modeling.py:312-380).  A warp streaming down rows k
+// therefore runs four row updates per iteration:
+//   forward:  A velocity k, A stress k-1, B velocity k-1, B stress k-2
+//   backward: A velocity k-1, A stress k-1, B velocity k-2, B stress k-2
+// and a task that writes rows [ia, ib) recomputes step A on one extra row
+// above and below (rows ia-1 .. ib) from the old state of rows ia-2 .. ib+1.
+// Rows -2 and nx+1 lie outside the padded shot block and read as zero; no
+// update touches a non-interior cell, so pad rows stay zero.
+//
+// Columns.  Lanes 0 and 31 carry VEC halo columns.  After step A only their
+// outermost column is wrong (its neighbour is outside the warp); after step
+// B the two outermost ones.  With VEC >= 2 every column that an owner lane
+// (1..30) reads is still exact, so the single-step decomposition is kept.
+//
+// Epilogues.  Step A's values are recorded (forward receivers,
+// _record_seismogram_kernel), snapshotted (forward) or correlated (backward
+// imaging) for rows [ia, ib) exactly like a single step; they are not
+// written back.  The finite check runs on step B only: the host never pairs
+// a step that is checked as step A, so a shot that fails stops at the step
+// where the reference stops.
+#pragma once
+#include <type_traits>
+
+#include "step_kernels.cuh"
+
+namespace rtm {
+
+template <int VEC>
+struct SigRow { float xx[VEC], zz[VEC], xz[VEC], yx[VEC], yz[VEC]; };
+template <int VEC>
+struct VelRow { float u[VEC], w[VEC], v[VEC]; };
+template <int VEC>
+struct MatRow { float lam[VEC], mu[VEC], mxz[VEC], myx[VEC], myz[VEC], sm[VEC]; };
+
+template <int VEC>
+__device__ __forceinline__ void zero_arr(float (&a)[VEC]) {
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) a[q] = 0.f;
+}
+
+template <int VEC>
+__device__ __forceinline__ void copy_arr(float (&d)[VEC], const float (&s)[VEC]) {
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) d[q] = s[q];
+}
+
+// Plain (coherent) vector load for the Kahan image: one thread may read a
+// cell again after writing it in the same launch (steps A and B both
+// imaging), which the read-only path (ld.global.nc) does not allow.
+template <int VEC>
+__device__ __forceinline__ void ldv_coherent(float (&v)[VEC], float *p) {
+    if constexpr (VEC == 4) {
+        const float4 t = *reinterpret_cast<float4 *>(p);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else if constexpr (VEC == 2) {
+        const float2 t = *reinterpret_cast<float2 *>(p);
+        v[0] = t.x; v[1] = t.y;
+    } else {
+        v[0] = *p;
+    }
+}
+
+template <int DIR, int MODE, int VEC>
+__global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
+    static_assert(VEC >= 2, "two steps per launch need two halo columns per side");
+    constexpr bool PSV = (MODE & 1) != 0;
+    constexpr bool SH = (MODE & 2) != 0;
+    constexpr int W = 30 * VEC;
+    using Sig = SigRow<VEC>;
+    using Vel = VelRow<VEC>;
+    using Mat = MatRow<VEC>;
+    const int lane = threadIdx.x & 31;
+    const int task = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (task >= p.n_work) return;
+    const int4 wk = p.work[task];
+    if (__ldg(p.flags + wk.x) != 0) return;  // this shot already failed: stop it
+    const ShotDev sh = p.shots[wk.x];
+    const int nx = sh.nx, nz = p.nz, P = p.pitch;
+    const int j0 = (wk.y & 0xFFFFF) * W;
+    const bool no_src = (wk.y >> 20) & 1, no_rec = (wk.y >> 21) & 1;
+    const int c0 = j0 - VEC + VEC * lane;
+    const bool owner = lane >= 1 && lane <= 30;
+    const int ia = wk.z, ib = wk.w;
+    const bool lane_in = c0 >= 1 && c0 + VEC - 1 <= nz - 2;
+    const bool lane_far = nz - 1 - (c0 + VEC - 1) >= p.fw;
+    auto all_in = [&](int i) { return lane_in && i >= 1 && i <= nx - 2; };
+    auto all_far = [&](int i) { return lane_far && i >= p.fw && nx - 1 - i >= p.fw; };
+    const long long soff = sh.state_off + (long long)(c0 + COL_OFF);
+    const long long moff = (long long)sh.x0 * P + (long long)(c0 + COL_OFF);
+    const float dt = p.dt, idx = p.inv_dx, idz = p.inv_dz;
+    const float sdt = DIR == 0 ? dt : -dt;
+    // rows -1 and nx are the zero pad rows of the shot block (and of the
+    // material window); rows beyond them are never read
+    auto row_ok = [&](int i) { return i >= -1 && i <= nx; };
+    auto LSt = [&](float (&v)[VEC], int f, int i) {
+        if (row_ok(i)) ldv<VEC>(v, p.sin[f] + soff + (long long)(i + 1) * P); else zero_arr<VEC>(v);
+    };
+    auto LMt = [&](float (&v)[VEC], int m, int i) {
+        if (row_ok(i)) ldv<VEC>(v, p.mat[m] + moff + (long long)(i + 1) * P); else zero_arr<VEC>(v);
+    };
+    auto load_sig = [&](int i, Sig &s) {
+        if constexpr (PSV) { LSt(s.xx, F_SXX, i); LSt(s.zz, F_SZZ, i); LSt(s.xz, F_SXZ, i); }
+        if constexpr (SH) { LSt(s.yx, F_SYX, i); LSt(s.yz, F_SYZ, i); }
+    };
+    auto load_vel = [&](int i, Vel &v) {
+        if constexpr (PSV) { LSt(v.u, F_U, i); LSt(v.w, F_W, i); }
+        if constexpr (SH) LSt(v.v, F_V, i);
+    };
+    auto load_ir = [&](int i, Vel &v) {
+        if constexpr (PSV) { LMt(v.u, M_IRU, i); LMt(v.w, M_IRW, i); }
+        if constexpr (SH) LMt(v.v, M_IR, i);
+    };
+    auto load_mat = [&](int i, Mat &m) {
+        if constexpr (PSV) { LMt(m.lam, M_LAM, i); LMt(m.mu, M_MU, i); LMt(m.mxz, M_MXZ, i); }
+        if constexpr (SH) { LMt(m.myx, M_MYX, i); LMt(m.myz, M_MYZ, i); }
+        if (p.surface) {
+            if (row_ok(i)) ldv<VEC>(m.sm, p.surface + moff + (long long)(i + 1) * P); else zero_arr<VEC>(m.sm);
+        } else {
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) m.sm[q] = 1.f;
+        }
+    };
+    auto cp_sig = [&](Sig &d, const Sig &s) {
+        if constexpr (PSV) { copy_arr<VEC>(d.xx, s.xx); copy_arr<VEC>(d.zz, s.zz); copy_arr<VEC>(d.xz, s.xz); }
+        if constexpr (SH) { copy_arr<VEC>(d.yx, s.yx); copy_arr<VEC>(d.yz, s.yz); }
+    };
+    auto cp_vel = [&](Vel &d, const Vel &s) {
+        if constexpr (PSV) { copy_arr<VEC>(d.u, s.u); copy_arr<VEC>(d.w, s.w); }
+        if constexpr (SH) copy_arr<VEC>(d.v, s.v);
+    };
+    auto cp_mat = [&](Mat &d, const Mat &s) {
+        if constexpr (PSV) { copy_arr<VEC>(d.lam, s.lam); copy_arr<VEC>(d.mu, s.mu); copy_arr<VEC>(d.mxz, s.mxz); }
+        if constexpr (SH) { copy_arr<VEC>(d.myx, s.myx); copy_arr<VEC>(d.myz, s.myz); }
+        copy_arr<VEC>(d.sm, s.sm);
+    };
+    auto zero_sig = [&](Sig &s) {
+        if constexpr (PSV) { zero_arr<VEC>(s.xx); zero_arr<VEC>(s.zz); zero_arr<VEC>(s.xz); }
+        if constexpr (SH) { zero_arr<VEC>(s.yx); zero_arr<VEC>(s.yz); }
+    };
+    auto zero_vel = [&](Vel &v) {
+        if constexpr (PSV) { zero_arr<VEC>(v.u); zero_arr<VEC>(v.w); }
+        if constexpr (SH) zero_arr<VEC>(v.v);
+    };
+
+    // Velocity update of row r (step time t), the arithmetic of step_kernel.
+    // Forward: sc = stress row r, sp = row r-1.  Backward: sc = row r+1,
+    // sp = row r.  vo = velocity of row r before the update.  FAST (every
+    // column of the lane interior) drops the interior select, nothing else.
+    auto vel_cells = [&](auto fast_tag, int r, const Sig &sc, const Sig &sp, const Vel &vo, const Vel &ir,
+                         Vel &out, float zz_nb, float xz_nb, float yz_nb) {
+        constexpr bool FAST = decltype(fast_tag)::value;
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            bool in = true;
+            if constexpr (!FAST) in = interior(r, c0 + q, nx, nz);
+            if constexpr (PSV) {
+                float du, dw;
+                if constexpr (DIR == 0) {
+                    const float sxz_jm = q > 0 ? sc.xz[q - 1] : xz_nb;
+                    const float szz_jm = q > 0 ? sc.zz[q - 1] : zz_nb;
+                    const float sxx_x = (sc.xx[q] - sp.xx[q]) * idx;  // fm:332
+                    const float szz_z = (sc.zz[q] - szz_jm) * idz;    // fm:333
+                    const float sxz_x = (sc.xz[q] - sp.xz[q]) * idx;  // fm:334
+                    const float sxz_z = (sc.xz[q] - sxz_jm) * idz;    // fm:335
+                    du = (sxx_x + sxz_z) * dt * ir.u[q];              // fm:339
+                    dw = (sxz_x + szz_z) * dt * ir.w[q];              // fm:340
+                } else {
+                    const float sxz_jp = q < VEC - 1 ? sp.xz[q + 1] : xz_nb;
+                    const float szz_jp = q < VEC - 1 ? sp.zz[q + 1] : zz_nb;
+                    const float sxx_x = (sc.xx[q] - sp.xx[q]) * idx;  // bm:333
+                    const float szz_z = (szz_jp - sp.zz[q]) * idz;    // bm:334
+                    const float sxz_x = (sc.xz[q] - sp.xz[q]) * idx;  // bm:335
+                    const float sxz_z = (sxz_jp - sp.xz[q]) * idz;    // bm:336
+                    du = -(sxx_x + sxz_z) * dt * ir.u[q];             // bm:340
+                    dw = -(sxz_x + szz_z) * dt * ir.w[q];             // bm:341
+                }
+                if constexpr (FAST) {
+                    out.u[q] = vo.u[q] + du;
+                    out.w[q] = vo.w[q] + dw;
+                } else {
+                    out.u[q] = in ? vo.u[q] + du : vo.u[q];
+                    out.w[q] = in ? vo.w[q] + dw : vo.w[q];
+                }
+            }
+            if constexpr (SH) {
+                float dv;
+                if constexpr (DIR == 0) {
+                    const float syz_jm = q > 0 ? sc.yz[q - 1] : yz_nb;
+                    const float syx_x = (sc.yx[q] - sp.yx[q]) * idx;  // fm:343
+                    const float syz_z = (sc.yz[q] - syz_jm) * idz;    // fm:344
+                    dv = (syx_x + syz_z) * dt * ir.v[q];              // fm:347
+                } else {
+                    const float syz_jp = q < VEC - 1 ? sp.yz[q + 1] : yz_nb;
+                    const float syx_x = (sc.yx[q] - sp.yx[q]) * idx;  // bm:343
+                    const float syz_z = (syz_jp - sp.yz[q]) * idz;    // bm:344
+                    dv = -(syx_x + syz_z) * dt * ir.v[q];             // bm:345
+                }
+                if constexpr (FAST) out.v[q] = vo.v[q] + dv;
+                else out.v[q] = in ? vo.v[q] + dv : vo.v[q];
+            }
+        }
+    };
+    auto vel_update = [&](int r, int t, const Sig &sc, const Sig &sp, const Vel &vo, const Vel &ir, Vel &out) {
+        // column neighbour: j-1 of row r (forward), j+1 of row r (backward)
+        float zz_nb = 0.f, xz_nb = 0.f, yz_nb = 0.f;
+        if constexpr (DIR == 0) {
+            if constexpr (PSV) {
+                zz_nb = __shfl_up_sync(FULL, sc.zz[VEC - 1], 1);
+                xz_nb = __shfl_up_sync(FULL, sc.xz[VEC - 1], 1);
+            }
+            if constexpr (SH) yz_nb = __shfl_up_sync(FULL, sc.yz[VEC - 1], 1);
+        } else {
+            if constexpr (PSV) {
+                zz_nb = __shfl_down_sync(FULL, sp.zz[0], 1);
+                xz_nb = __shfl_down_sync(FULL, sp.xz[0], 1);
+            }
+            if constexpr (SH) yz_nb = __shfl_down_sync(FULL, sp.yz[0], 1);
+        }
+        if (all_in(r)) vel_cells(std::true_type{}, r, sc, sp, vo, ir, out, zz_nb, xz_nb, yz_nb);
+        else vel_cells(std::false_type{}, r, sc, sp, vo, ir, out, zz_nb, xz_nb, yz_nb);
+        // point injection at time t: forward sources (fm:421-443), backward
+        // observed data (bm:452-460); halo lanes too, so halo cells are exact
+        if (r < 0 || r >= nx) return;
+        if constexpr (DIR == 0) {
+            if (no_src) return;
+            const int e0 = __ldg(p.src_ptr + sh.src_row0 + r), e1 = __ldg(p.src_ptr + sh.src_row0 + r + 1);
+            for (int e = e0; e < e1; ++e) {
+                const int2 en = __ldg(p.src_ent + e);
+                const int q = en.x - c0;
+                if (q < 0 || q >= VEC) continue;
+                const bool in = interior(r, en.x, nx, nz);
+                const float f = p.src_factor;
+                const size_t ti = (size_t)en.y * p.nt + t;
+#pragma unroll
+                for (int qq = 0; qq < VEC; ++qq) {
+                    if (qq != q) continue;
+                    if constexpr (PSV) {
+                        out.u[qq] += __ldg(p.wav[0] + ti) * f * (in ? ir.u[qq] : __int_as_float(0x7f800000));
+                        out.w[qq] += __ldg(p.wav[2] + ti) * f * (in ? ir.w[qq] : __int_as_float(0x7f800000));
+                    }
+                    if constexpr (SH) out.v[qq] += __ldg(p.wav[1] + ti) * f * ir.v[qq];
+                }
+            }
+        } else {
+            if (no_rec) return;
+            const int e0 = __ldg(p.rec_ptr + sh.rec_row0 + r), e1 = __ldg(p.rec_ptr + sh.rec_row0 + r + 1);
+            for (int e = e0; e < e1; ++e) {
+                const int2 en = __ldg(p.rec_ent + e);
+                const int q = en.x - c0;
+                if (q < 0 || q >= VEC) continue;
+                const size_t ti = (size_t)t * p.nrec_total + en.y;
+#pragma unroll
+                for (int qq = 0; qq < VEC; ++qq) {
+                    if (qq != q) continue;
+                    if constexpr (PSV) {
+                        out.u[qq] += __ldg(p.obs[0] + ti);
+                        out.w[qq] += __ldg(p.obs[2] + ti);
+                    }
+                    if constexpr (SH) out.v[qq] += __ldg(p.obs[1] + ti);
+                }
+            }
+        }
+    };
+
+    // Stress update of row r, then absorbing and the surface mask of the
+    // next step: va = new velocity of row r, vb = of row r+1 (forward) or
+    // r-1 (backward), base = stress of row r before the step.  FAST (every
+    // column of the lane interior, outside the sponge, no topography mask)
+    // drops the interior select and the multiplications by a coefficient of
+    // exactly 1.0, which leave every value unchanged.
+    auto stress_cells = [&](auto fast_tag, int r, const Vel &va, const Vel &vb, const Sig &base, const Mat &m,
+                            Sig &os, Vel &ov, float nu, float nw, float nv) {
+        constexpr bool FAST = decltype(fast_tag)::value;
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            const int j = c0 + q;
+            bool in = true;
+            float cr = 1.0f;
+            if constexpr (!FAST) {
+                in = interior(r, j, nx, nz);
+                cr = sponge_coef(p, nx, r, j);
+            }
+            if constexpr (PSV) {
+                float u_x, u_z, w_x, w_z;
+                if constexpr (DIR == 0) {
+                    const float uj = q < VEC - 1 ? va.u[q + 1] : nu;
+                    const float wj = q < VEC - 1 ? va.w[q + 1] : nw;
+                    u_x = (vb.u[q] - va.u[q]) * idx;   // fm:369
+                    u_z = (uj - va.u[q]) * idz;        // fm:370
+                    w_x = (vb.w[q] - va.w[q]) * idx;   // fm:371
+                    w_z = (wj - va.w[q]) * idz;        // fm:372
+                } else {
+                    const float uj = q > 0 ? va.u[q - 1] : nu;
+                    const float wj = q > 0 ? va.w[q - 1] : nw;
+                    u_x = (va.u[q] - vb.u[q]) * idx;   // bm:366
+                    u_z = (va.u[q] - uj) * idz;        // bm:367
+                    w_x = (va.w[q] - vb.w[q]) * idx;   // bm:368
+                    w_z = (va.w[q] - wj) * idz;        // bm:369
+                }
+                const float div = u_x + w_z;
+                const float sxx = base.xx[q] + sdt * (m.lam[q] * div + 2.0f * m.mu[q] * u_x);
+                const float szz = base.zz[q] + sdt * (m.lam[q] * div + 2.0f * m.mu[q] * w_z);
+                const float sxz = base.xz[q] + sdt * m.mxz[q] * (u_z + w_x);
+                if constexpr (FAST) {
+                    os.xx[q] = sxx;
+                    os.zz[q] = szz;
+                    os.xz[q] = sxz;
+                    ov.u[q] = va.u[q];
+                    ov.w[q] = va.w[q];
+                } else {
+                    os.xx[q] = cr * (in ? sxx : base.xx[q]);
+                    os.zz[q] = (cr * (in ? szz : base.zz[q])) * m.sm[q];
+                    os.xz[q] = (cr * (in ? sxz : base.xz[q])) * m.sm[q];
+                    ov.u[q] = cr * va.u[q];
+                    ov.w[q] = cr * va.w[q];
+                }
+            }
+            if constexpr (SH) {
+                float v_x, v_z;
+                if constexpr (DIR == 0) {
+                    const float vj = q < VEC - 1 ? va.v[q + 1] : nv;
+                    v_x = (vb.v[q] - va.v[q]) * idx;   // fm:381
+                    v_z = (vj - va.v[q]) * idz;        // fm:382
+                } else {
+                    const float vj = q > 0 ? va.v[q - 1] : nv;
+                    v_x = (va.v[q] - vb.v[q]) * idx;   // bm:377
+                    v_z = (va.v[q] - vj) * idz;        // bm:378
+                }
+                const float syx = base.yx[q] + sdt * m.myx[q] * v_x;
+                const float syz = base.yz[q] + sdt * m.myz[q] * v_z;
+                if constexpr (FAST) {
+                    os.yx[q] = syx;
+                    os.yz[q] = syz;
+                    ov.v[q] = va.v[q];
+                } else {
+                    os.yx[q] = cr * (in ? syx : base.yx[q]);
+                    os.yz[q] = (cr * (in ? syz : base.yz[q])) * m.sm[q];
+                    ov.v[q] = cr * va.v[q];
+                }
+            }
+        }
+    };
+    auto stress_update = [&](int r, const Vel &va, const Vel &vb, const Sig &base, const Mat &m, Sig &os,
+                             Vel &ov) {
+        float nu = 0.f, nw = 0.f, nv = 0.f;
+        if constexpr (DIR == 0) {
+            if constexpr (PSV) { nu = __shfl_down_sync(FULL, va.u[0], 1); nw = __shfl_down_sync(FULL, va.w[0], 1); }
+            if constexpr (SH) nv = __shfl_down_sync(FULL, va.v[0], 1);
+        } else {
+            if constexpr (PSV) { nu = __shfl_up_sync(FULL, va.u[VEC - 1], 1); nw = __shfl_up_sync(FULL, va.w[VEC - 1], 1); }
+            if constexpr (SH) nv = __shfl_up_sync(FULL, va.v[VEC - 1], 1);
+        }
+        if (all_in(r) && all_far(r) && p.surface == nullptr)
+            stress_cells(std::true_type{}, r, va, vb, base, m, os, ov, nu, nw, nv);
+        else
+            stress_cells(std::false_type{}, r, va, vb, base, m, os, ov, nu, nw, nv);
+    };
+
+    // Per-step outputs of an absorbed velocity row r (owner lanes, r in
+    // [ia, ib)): forward receivers at time t and snapshot slot k, backward
+    // Kahan imaging against snapshot slot k.
+    auto epilogue = [&](int r, int t, int k, const Vel &v) {
+        if constexpr (DIR == 0) {
+            const int e0 = no_rec ? 0 : __ldg(p.rec_ptr + sh.rec_row0 + r);
+            const int e1 = no_rec ? 0 : __ldg(p.rec_ptr + sh.rec_row0 + r + 1);
+            for (int e = e0; e < e1; ++e) {
+                const int2 en = __ldg(p.rec_ent + e);
+                const int q = en.x - c0;
+                if (q < 0 || q >= VEC) continue;
+                const size_t ti = (size_t)t * p.nrec_total + en.y;
+#pragma unroll
+                for (int qq = 0; qq < VEC; ++qq) {
+                    if (qq != q) continue;
+                    if constexpr (PSV) { p.seis[0][ti] = v.u[qq]; p.seis[2][ti] = v.w[qq]; }
+                    if constexpr (SH) p.seis[1][ti] = v.v[qq];
+                }
+            }
+            if (k >= 0) {
+                const long long o = ((long long)p.nsnap * sh.row_off + (long long)k * nx + r) * P + c0 + COL_OFF;
+                if constexpr (PSV) { stv<VEC>(p.snap[0] + o, v.u); stv<VEC>(p.snap[2] + o, v.w); }
+                if constexpr (SH) stv<VEC>(p.snap[1] + o, v.v);
+            }
+        } else {
+            if (k >= 0) {
+                const long long o = ((long long)p.nsnap * sh.row_off + (long long)k * nx + r) * P + c0 + COL_OFF;
+                const long long io = (sh.row_off + r) * (long long)P + c0 + COL_OFF;
+                auto image = [&](int c, const float (&ov)[VEC]) {
+                    float s[VEC], sum[VEC], cmp[VEC];
+                    ldv<VEC>(s, p.snap[c] + o);
+                    ldv_coherent<VEC>(sum, p.img[c] + io);
+                    ldv_coherent<VEC>(cmp, p.imgc[c] + io);
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) kahan_add(sum[q], cmp[q], __fmul_rn(s[q], ov[q]));
+                    stv<VEC>(p.img[c] + io, sum);
+                    stv<VEC>(p.imgc[c] + io, cmp);
+                };
+                if constexpr (PSV) { image(0, v.u); image(2, v.w); }
+                if constexpr (SH) image(1, v.v);
+            }
+        }
+    };
+
+    int code = 0;
+    auto check_row = [&](const Vel &v) {
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            if constexpr (PSV) {
+                code = max(code, bad_code(v.u[q], p.code_base));
+                code = max(code, bad_code(v.w[q], p.code_base + 2));
+            }
+            if constexpr (SH) code = max(code, bad_code(v.v[q], p.code_base + 1));
+        }
+    };
+    // step B's stress and absorbed velocity of row r: store, outputs, check
+    auto finish_b = [&](int r, const Sig &os, const Vel &ov) {
+        if (!owner) return;
+        const long long so = soff + (long long)(r + 1) * P;
+        if constexpr (PSV) {
+            stv<VEC>(p.sout[F_SXX] + so, os.xx);
+            stv<VEC>(p.sout[F_SZZ] + so, os.zz);
+            stv<VEC>(p.sout[F_SXZ] + so, os.xz);
+            stv<VEC>(p.sout[F_U] + so, ov.u);
+            stv<VEC>(p.sout[F_W] + so, ov.w);
+        }
+        if constexpr (SH) {
+            stv<VEC>(p.sout[F_SYX] + so, os.yx);
+            stv<VEC>(p.sout[F_SYZ] + so, os.yz);
+            stv<VEC>(p.sout[F_V] + so, ov.v);
+        }
+        epilogue(r, p.it2, p.snap_k2, ov);
+        if (p.check) check_row(ov);
+    };
+
+    const int tA = p.it, tB = p.it2;
+    // rolling rows (see the header comment for which row each holds)
+    Sig so_p, so_c, sa_p, sa_c, s_out, n_so;
+    Vel va_p, va_c, vb_p, vb_c, vo, ir_p, ir_c, vabs_c, v_out, n_vo, n_ir;
+    Mat m_p, m_c, n_m;
+    zero_sig(sa_p); zero_sig(sa_c);
+    zero_vel(va_p); zero_vel(vb_p); zero_vel(vabs_c);
+    load_sig(ia - 2, so_p);
+
+    if constexpr (DIR == 0) {
+        // iteration k: A velocity k, A stress k-1, B velocity k-1, B stress k-2
+        // prefetched per iteration: old stress, old velocity, 1/rho of row k+1; material of row k
+        load_sig(ia - 1, n_so);
+        load_vel(ia - 1, n_vo);
+        load_ir(ia - 1, n_ir);
+        load_mat(ia - 2, n_m);
+        for (int k = ia - 1; k <= ib + 1; ++k) {
+            cp_sig(so_c, n_so);
+            cp_vel(vo, n_vo);
+            cp_vel(ir_c, n_ir);
+            cp_mat(m_c, n_m);  // row k-1
+            if (k <= ib) {
+                load_sig(k + 1, n_so);
+                load_vel(k + 1, n_vo);
+                load_ir(k + 1, n_ir);
+                load_mat(k, n_m);
+            }
+            vel_update(k, tA, so_c, so_p, vo, ir_c, va_c);
+            if (k >= ia) {
+                stress_update(k - 1, va_p, va_c, so_p, m_c, sa_c, vabs_c);
+                if (owner && k - 1 >= ia && k - 1 < ib) epilogue(k - 1, tA, p.snap_k, vabs_c);
+            }
+            if (k >= ia + 1) vel_update(k - 1, tB, sa_c, sa_p, vabs_c, ir_p, vb_c);
+            if (k >= ia + 2) {
+                stress_update(k - 2, vb_p, vb_c, sa_p, m_p, s_out, v_out);
+                finish_b(k - 2, s_out, v_out);
+            }
+            cp_sig(so_p, so_c);
+            cp_vel(va_p, va_c);
+            cp_sig(sa_p, sa_c);
+            cp_vel(vb_p, vb_c);
+            cp_vel(ir_p, ir_c);
+            cp_mat(m_p, m_c);
+        }
+    } else {
+        // iteration k: A velocity k-1, A stress k-1, B velocity k-2, B stress k-2
+        // prefetched per iteration: old stress of row k+1; old velocity, 1/rho, material of row k
+        Vel vabs_p;
+        zero_vel(vabs_p);
+        load_sig(ia - 1, n_so);
+        load_vel(ia - 2, n_vo);
+        load_ir(ia - 2, n_ir);
+        load_mat(ia - 2, n_m);
+        for (int k = ia - 1; k <= ib + 1; ++k) {
+            cp_sig(so_c, n_so);   // row k
+            cp_vel(vo, n_vo);     // row k-1
+            cp_vel(ir_c, n_ir);   // row k-1
+            cp_mat(m_c, n_m);     // row k-1
+            if (k <= ib) {
+                load_sig(k + 1, n_so);
+                load_vel(k, n_vo);
+                load_ir(k, n_ir);
+                load_mat(k, n_m);
+            }
+            vel_update(k - 1, tA, so_c, so_p, vo, ir_c, va_c);
+            if (k >= ia) {
+                stress_update(k - 1, va_c, va_p, so_p, m_c, sa_c, vabs_c);
+                if (owner && k - 1 >= ia && k - 1 < ib) epilogue(k - 1, tA, p.snap_k, vabs_c);
+            }
+            if (k >= ia + 1) vel_update(k - 2, tB, sa_c, sa_p, vabs_p, ir_p, vb_c);
+            if (k >= ia + 2) {
+                stress_update(k - 2, vb_c, vb_p, sa_p, m_p, s_out, v_out);
+                finish_b(k - 2, s_out, v_out);
+            }
+            cp_sig(so_p, so_c);
+            cp_vel(va_p, va_c);
+            cp_sig(sa_p, sa_c);
+            cp_vel(vabs_p, vabs_c);
+            cp_vel(vb_p, vb_c);
+            cp_vel(ir_p, ir_c);
+            cp_mat(m_p, m_c);
+        }
+    }
+    if (p.check) {
+        code = __reduce_max_sync(FULL, code);
+        if (lane == 0 && code > 0) atomicMax(p.flags + wk.x, code);
+    }
+}
+
+}  // namespace rtm

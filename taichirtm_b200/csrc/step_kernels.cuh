@@ -84,6 +84,7 @@ struct StepParams {
     int code_base;           // 1 forward, 4 backward
     int *flags;              // per shot status
     int it;                  // forward: step it; backward: reversed time t
+    int it2, snap_k2;        // two-step launches: time and snapshot slot of the second step
 };
 
 template <int VEC>

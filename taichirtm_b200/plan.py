@@ -65,7 +65,7 @@ class Plan:
             arr[k] = _lib.RtmShot(s.x0, s.nx, len(s.src), _i32p(s.src), len(s.rec), _i32p(s.rec))
         t = tune or {}
         tn = _lib.RtmTune(int(t.get("vec", 0)), int(t.get("rows", 0)), int(t.get("warps", 0)),
-                          int(t.get("prefetch", -1)), int(t.get("graphs", 0)))
+                          int(t.get("prefetch", -1)), int(t.get("graphs", 0)), int(t.get("tsteps", 0)))
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             check(L.rtm_plan_create(ctypes.byref(g), len(self.shots), arr, ctypes.byref(tn),
