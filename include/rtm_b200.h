@@ -141,6 +141,22 @@ int rtm_backward(rtm_plan *plan, const float *obs, const float *snap_u, const fl
                  float *image, double *stack, int check_interval, int32_t *flags,
                  rtm_stream_t stream);
 
+/* Source-normalised zero-lag cross-correlation: the imaging condition that
+ * the reference advertises beside plain cross-correlation but leaves
+ * unimplemented (it accepts and ignores run_calc's `method`,
+ * backward_modeling.py:505).  rtm_backward, then each shot's image is divided,
+ * component by component, by that shot's source illumination
+ *     I_c(i, j) = sum over the imaging steps of snapshot_c(i, j)^2
+ * (the snapshots and steps the correlation used), stabilised by eps times
+ * the shot's maximum illumination:
+ *     image_c = xcorr_c / (I_c + eps * max I_c)      (0 where the divisor is 0).
+ * Shots are normalised one by one before the stack.  Arguments as
+ * rtm_backward, plus eps >= 0.  No reference counterpart (extension). */
+int rtm_backward_normalized(rtm_plan *plan, const float *obs, const float *snap_u,
+                            const float *snap_v, const float *snap_w, const int32_t *isnaps,
+                            int num_snaps, int isnap, float eps, float *image, double *stack,
+                            int check_interval, int32_t *flags, rtm_stream_t stream);
+
 /* ---- Exact adjoint (FWI gradients).  No counterpart in the reference, whose
  * backward propagation (backward_modeling.py:312-380) is not the adjoint of
  * its forward; these differentiate the forward step of

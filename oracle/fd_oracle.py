@@ -364,3 +364,35 @@ def estimate_velocity(array, receiver_loc, source_loc, fs, vmin, vmax, vstep=10)
             sum_max = sum_v
             v_est = v
     return float(v_est)
+
+
+def imaging_slots(nt, isnap, isnaps, num_snaps):
+    """Snapshot slots the cross-correlation uses, in backward order: slot
+    k = t // isnap - 1 at every reversed time t > 0 with t % isnap == 0 and
+    isnaps[k] == t (backward_modeling.py:556-564)."""
+    out = []
+    for it in range(nt):
+        t = (nt - 1) - it
+        if t > 0 and t % isnap == 0:
+            k = t // isnap - 1
+            if 0 <= k < num_snaps and int(isnaps[k]) == t:
+                out.append(k)
+    return out
+
+
+def source_normalized(img, snaps, slots, eps):
+    """Source-normalised zero-lag cross-correlation.  No reference
+    counterpart: the reference accepts an imaging ``method`` and ignores it
+    (backward_modeling.py:505).  The definition restated here: per component c,
+    I_c = sum over the used snapshot slots of snapshot_c^2 (FP64) and
+    image_c = xcorr_c / (I_c + eps * max I_c), 0 where that divisor is 0.
+    ``img`` is (3, nx, nz), ``snaps`` (3, nx, nz, nsnap)."""
+    out = np.zeros(np.shape(img), np.float64)
+    for c in range(3):
+        ill = np.zeros(np.shape(img)[1:], np.float64)
+        for k in slots:
+            s = np.asarray(snaps[c, :, :, k], np.float64)
+            ill += s * s
+        d = ill + eps * ill.max()
+        out[c] = np.where(d > 0, np.asarray(img[c], np.float64) / np.where(d > 0, d, 1.0), 0.0)
+    return out

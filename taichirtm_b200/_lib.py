@@ -73,6 +73,8 @@ def lib():
     _sig(L, "rtm_plan_set_model", c_int, vp, vp, vp, vp, vp, vp)
     _sig(L, "rtm_forward", c_int, vp, vp, vp, c_int, c_int, vp, vp, vp, I32P, c_int, I32P, vp)
     _sig(L, "rtm_backward", c_int, vp, vp, vp, vp, vp, I32P, c_int, c_int, vp, vp, c_int, I32P, vp)
+    _sig(L, "rtm_backward_normalized", c_int, vp, vp, vp, vp, vp, I32P, c_int, c_int, ctypes.c_float, vp, vp,
+         c_int, I32P, vp)
     _sig(L, "rtm_plan_state_floats", c_size, vp)
     _sig(L, "rtm_plan_num_checkpoints", c_int, vp, c_int)
     _sig(L, "rtm_plan_checkpoint_bytes", c_size, vp, c_int, c_int)

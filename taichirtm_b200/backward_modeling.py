@@ -91,15 +91,22 @@ class BackwardModeling:
     def run_calc(self, import_fwdata_u, import_fwdata_v, import_fwdata_w, isnaps_field,
                  num_snaps: int, isnap_interval: int, method: str = "cross_correlation",
                  display_callback: Optional[Callable] = None,
-                 stability_check_interval: int = 100) -> int:
+                 stability_check_interval: int = 100, *, normalization_eps: float = 1e-3) -> int:
         """BackwardModeling.run_calc (backward_modeling.py:498-579): 0 on
-        success, 4 / 5 / 6 when u / v / w became non-finite.  ``method`` is
-        accepted and, like the reference, not used (bm:505, 539-579)."""
+        success, 4 / 5 / 6 when u / v / w became non-finite.
+
+        ``method``: "cross_correlation" (default) and any name the reference
+        accepts without using it ("convolution", bm:505) give the reference's
+        zero-lag cross-correlation; "source_normalized" (an extension) divides
+        the image by the source illumination sum_t snapshot^2 plus
+        ``normalization_eps`` times its maximum."""
         self._make_plan(self.modes)
         isnaps = to_numpy(isnaps_field, np.int32).reshape(-1)[: max(int(num_snaps), 0)]
         snaps = self._snapshot_buffers((import_fwdata_u, import_fwdata_v, import_fwdata_w), int(num_snaps))
+        eps = float(normalization_eps) if method == "source_normalized" else None
         flags, img, _ = self.plan.backward(self._obs, snaps, isnaps, int(num_snaps), int(isnap_interval),
-                                           check_interval=stability_check_interval, image=True)
+                                           check_interval=stability_check_interval, image=True,
+                                           normalize_eps=eps)
         self._img = img
         if display_callback is not None:
             im = img.cpu().numpy()

@@ -69,7 +69,8 @@ class BatchedRTM:
         w = to_tensor(wavelets, torch.float32, self.device)
         return self.plan.forward(w, save=save, isnap=isnap, check_interval=check_interval)
 
-    def migrate(self, wavelets, observed, isnap=10, check_interval=100, stack=None, checkpoint=None):
+    def migrate(self, wavelets, observed, isnap=10, check_interval=100, stack=None, checkpoint=None,
+                method="cross_correlation", normalization_eps=1e-3):
         """Forward with snapshots, backward with imaging, FP64 stack of every
         shot's image on the global grid.  Returns (forward flags, backward
         flags, stack (3, nx, nz) float64 on the device).
@@ -78,16 +79,23 @@ class BatchedRTM:
         wavefield every K steps instead of snapshots and recomputes the
         forward wavefield segment by segment during the backward pass (P-SV):
         memory ~ (nt/K) x 5 fields instead of (nt/isnap) x 2, one extra
-        forward pass of compute; FP32 checkpoints give the same image bits."""
+        forward pass of compute; FP32 checkpoints give the same image bits.
+
+        ``method="source_normalized"`` divides every shot's image by its source
+        illumination (sum of squared snapshots over the imaging steps) plus
+        ``normalization_eps`` times its maximum before stacking (snapshot path)."""
         w = to_tensor(wavelets, torch.float32, self.device)
         o = to_tensor(observed, torch.float32, self.device)
         if checkpoint:
+            if method == "source_normalized":
+                raise ValueError("source_normalized imaging needs the snapshot path (checkpoint=None)")
             return self._migrate_checkpointed(w, o, isnap, check_interval, stack, checkpoint)
         ff, _, snaps, isnaps = self.plan.forward(w, save=True, isnap=isnap, check_interval=check_interval)
         if stack is None:
             stack = torch.zeros((3, self.nx, self.nz), dtype=torch.float64, device=self.device)
         fb, _, _ = self.plan.backward(o, snaps, isnaps, len(isnaps), isnap, check_interval=check_interval,
-                                      image=False, stack=stack)
+                                      image=False, stack=stack,
+                                      normalize_eps=normalization_eps if method == "source_normalized" else None)
         del snaps
         return ff, fb, stack
 

@@ -17,7 +17,8 @@
 //   alpha' = c a_n + Ds^T ubar                    (= dJ/dv'_n)
 //   gamma  = I dt B alpha'
 //   b_{n-1} = beta' + Dv^T gamma,   a_{n-1} = alpha' + R^T g_{n-1}
-// and the model gradients accumulated over n:
+// and the model gradients accumulated over n (FP32 partials folded into
+// Kahan pairs every GRAD_FOLD_STEPS steps):
 //   dJ/dlam += dt (beta_xx + beta_zz) div(v'_n),  dJ/dmu += 2 dt (beta_xx u_x + beta_zz w_z),
 //   dJ/dmxz += dt beta_xz (u_z + w_x),            dJ/dB   += alpha' I dt Dv(S_{n-1})
 //                                                           (+ alpha' w_n f at interior sources),
@@ -55,8 +56,7 @@ struct AdjParams {
     const int2 *rec_ent;
     int nrec_total;
     const float *resid[3];    // time-major (nt, nrec_total): dJ/d(seismogram)
-    float *grad[NGRAD];       // per shot [row_off + i][pitch], Kahan sums
-    float *gradc[NGRAD];      // Kahan compensations
+    float *gpart[NGRAD];      // per shot [row_off + i][pitch]: FP32 partial sums since the last fold
     float *gwav[3];           // time-major (nt, nsrc_total) dJ/d(wavelet), or null
     int nsrc_total;
     int n;                    // forward step reversed by this launch
@@ -83,6 +83,33 @@ static __global__ void inject_last_resid_kernel(const ShotDev *__restrict__ shot
             au[o] += resid_t[t];
             aw[o] += resid_t[2 * plane + t];
         }
+}
+
+// Gradient accumulation: every adjoint step adds its contribution to a plain
+// FP32 partial sum (one read and one write per cell and gradient); every
+// GRAD_FOLD_STEPS reversed steps, counted on the global step number n (so
+// the grouping does not depend on the checkpoint interval), the partials are
+// folded into a Kahan pair (sum, comp) and cleared.  A partial holds at most
+// 64 terms, so its relative rounding error stays below 64 x 2^-24.
+constexpr int GRAD_FOLD_STEPS = 64;
+
+struct GradFold {
+    float *part[NGRAD], *sum[NGRAD], *comp[NGRAD];
+    long long n;  // floats per array
+};
+
+static __global__ void grad_fold_kernel(const GradFold f) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < f.n;
+         i += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int g = 0; g < NGRAD; ++g) {
+            float s = f.sum[g][i], c = f.comp[g][i];
+            kahan_add(s, c, f.part[g][i]);
+            f.sum[g][i] = s;
+            f.comp[g][i] = c;
+            f.part[g][i] = 0.f;
+        }
+    }
 }
 
 // Same coefficient as sponge_coef (forward_modeling.py:203-235 loop order).
@@ -133,24 +160,54 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
         up_p[q] = wp_p[q] = au_p[q] = aw_p[q] = gu_p[q] = gw_p[q] = dvu_p[q] = dvw_p[q] = 0.f;
     }
 
-    for (int k = ia - 1; k <= ib; ++k) {
-        // ---- pointwise quantities of row k
+    // Inputs of one row, loaded one iteration ahead (software pipelining:
+    // the loads of row k+1 are in flight while row k is computed).
+    struct Row {
         float sxx[VEC], szz[VEC], sxz[VEC], bxx[VEC], bzz[VEC], bxz[VEC];
         float lam[VEC], mu[VEC], mxz[VEC], sm[VEC];
-        ldv<VEC>(sxx, F(A_SXX, k));
-        ldv<VEC>(szz, F(A_SZZ, k));
-        ldv<VEC>(sxz, F(A_SXZ, k));
-        ldv<VEC>(bxx, A(A_SXX, k));
-        ldv<VEC>(bzz, A(A_SZZ, k));
-        ldv<VEC>(bxz, A(A_SXZ, k));
-        ldv<VEC>(lam, M(M_LAM, k));
-        ldv<VEC>(mu, M(M_MU, k));
-        ldv<VEC>(mxz, M(M_MXZ, k));
+        float u[VEC], w[VEC], au[VEC], aw[VEC], bu[VEC], bw[VEC];  // rows >= ia only
+    };
+    auto load_row = [&](int i, Row &x, bool vel) {
+        ldv<VEC>(x.sxx, F(A_SXX, i));
+        ldv<VEC>(x.szz, F(A_SZZ, i));
+        ldv<VEC>(x.sxz, F(A_SXZ, i));
+        ldv<VEC>(x.bxx, A(A_SXX, i));
+        ldv<VEC>(x.bzz, A(A_SZZ, i));
+        ldv<VEC>(x.bxz, A(A_SXZ, i));
+        ldv<VEC>(x.lam, M(M_LAM, i));
+        ldv<VEC>(x.mu, M(M_MU, i));
+        ldv<VEC>(x.mxz, M(M_MXZ, i));
         if (p.surface) {
-            ldv<VEC>(sm, p.surface + moff + (long long)(k + 1) * P);
+            ldv<VEC>(x.sm, p.surface + moff + (long long)(i + 1) * P);
         } else {
 #pragma unroll
-            for (int q = 0; q < VEC; ++q) sm[q] = 1.f;
+            for (int q = 0; q < VEC; ++q) x.sm[q] = 1.f;
+        }
+        if (vel) {
+            ldv<VEC>(x.u, F(A_U, i));
+            ldv<VEC>(x.w, F(A_W, i));
+            ldv<VEC>(x.au, A(A_U, i));
+            ldv<VEC>(x.aw, A(A_W, i));
+            ldv<VEC>(x.bu, M(M_IRU, i));
+            ldv<VEC>(x.bw, M(M_IRW, i));
+        } else {
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) x.u[q] = x.w[q] = x.au[q] = x.aw[q] = x.bu[q] = x.bw[q] = 0.f;
+        }
+    };
+    Row nxt;
+    load_row(ia - 1, nxt, false);  // row ia-1 needs no velocity inputs
+    for (int k = ia - 1; k <= ib; ++k) {
+        // ---- pointwise quantities of row k
+        const Row cur = nxt;
+        if (k < ib) load_row(k + 1, nxt, true);
+        float sxx[VEC], szz[VEC], sxz[VEC], bxx[VEC], bzz[VEC], bxz[VEC];
+        float lam[VEC], mu[VEC], mxz[VEC], sm[VEC];
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) {
+            sxx[q] = cur.sxx[q]; szz[q] = cur.szz[q]; sxz[q] = cur.sxz[q];
+            bxx[q] = cur.bxx[q]; bzz[q] = cur.bzz[q]; bxz[q] = cur.bxz[q];
+            lam[q] = cur.lam[q]; mu[q] = cur.mu[q]; mxz[q] = cur.mxz[q]; sm[q] = cur.sm[q];
         }
         float cc[VEC], ins[VEC], uxb[VEC], wzb[VEC], xzb[VEC];
 #pragma unroll
@@ -178,13 +235,12 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
         const float xzb_m = __shfl_up_sync(FULL, xzb[VEC - 1], 1);
         const float wzb_m = __shfl_up_sync(FULL, wzb[VEC - 1], 1);
         if (k >= ia) {
-            float u[VEC], w[VEC], bu[VEC], bw[VEC], au_in[VEC], aw_in[VEC];
-            ldv<VEC>(u, F(A_U, k));
-            ldv<VEC>(w, F(A_W, k));
-            ldv<VEC>(au_in, A(A_U, k));
-            ldv<VEC>(aw_in, A(A_W, k));
-            ldv<VEC>(bu, M(M_IRU, k));
-            ldv<VEC>(bw, M(M_IRW, k));
+            const float(&u)[VEC] = cur.u;
+            const float(&w)[VEC] = cur.w;
+            const float(&au_in)[VEC] = cur.au;
+            const float(&aw_in)[VEC] = cur.aw;
+            const float(&bu)[VEC] = cur.bu;
+            const float(&bw)[VEC] = cur.bw;
 #pragma unroll
             for (int q = 0; q < VEC; ++q) {
                 const float sxz_jm = q > 0 ? sxz[q - 1] : sxz_m;
@@ -303,13 +359,11 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
                 stv<VEC>(p.aout[A_SXZ] + so, oxz);
                 const long long go = (sh.row_off + r) * (long long)P + c0 + COL_OFF;
                 auto acc = [&](int gi, const float (&d)[VEC]) {
-                    float s[VEC], cmp[VEC];
-                    ldv<VEC>(s, p.grad[gi] + go);
-                    ldv<VEC>(cmp, p.gradc[gi] + go);
+                    float s[VEC];
+                    ldv<VEC>(s, p.gpart[gi] + go);
 #pragma unroll
-                    for (int q = 0; q < VEC; ++q) kahan_add(s[q], cmp[q], d[q]);
-                    stv<VEC>(p.grad[gi] + go, s);
-                    stv<VEC>(p.gradc[gi] + go, cmp);
+                    for (int q = 0; q < VEC; ++q) s[q] = __fadd_rn(s[q], d[q]);
+                    stv<VEC>(p.gpart[gi] + go, s);
                 };
                 acc(G_LAM, dl);
                 acc(G_MU, dm);

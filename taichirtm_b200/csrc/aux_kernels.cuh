@@ -69,16 +69,31 @@ static __global__ void transpose_kernel(const float *__restrict__ in, float *__r
     }
 }
 
+// Optional source-illumination normalisation of the images: per shot cell
+// I (FP64, indexed like the image), per shot the bits of max I (a
+// non-negative double, so its bits order like its value), and eps.
+struct IllumNorm {
+    const double *illum = nullptr;             // nullptr: plain cross-correlation
+    const unsigned long long *imax = nullptr;  // per shot
+    double eps = 0.0;
+};
+
+__device__ __forceinline__ double normalise(double xc, const IllumNorm &nm, long long o, int shot) {
+    if (!nm.illum) return xc;
+    const double d = nm.illum[o] + nm.eps * __longlong_as_double((long long)nm.imax[shot]);
+    return d > 0.0 ? xc / d : 0.0;
+}
+
 // Per-shot Kahan image (sum, comp) -> compact (nx, nz) float image of one shot.
 static __global__ void image_out_kernel(const float *__restrict__ sum, const float *__restrict__ comp,
                                  float *__restrict__ out, long long row_off, int nx, int nz,
-                                 int pitch) {
+                                 int pitch, IllumNorm nm = IllumNorm()) {
     const long long n = (long long)nx * nz;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
          idx += (long long)gridDim.x * blockDim.x) {
         const int i = (int)(idx / nz), j = (int)(idx % nz);
         const long long o = (row_off + i) * pitch + j + COL_OFF;
-        out[idx] = (float)((double)sum[o] - (double)comp[o]);
+        out[idx] = (float)normalise((double)sum[o] - (double)comp[o], nm, o, 0);
     }
 }
 
@@ -87,7 +102,7 @@ static __global__ void image_out_kernel(const float *__restrict__ sum, const flo
 // shot order (deterministic).
 static __global__ void stack_kernel(const float *__restrict__ sum, const float *__restrict__ comp,
                              double *__restrict__ stack, const ShotDev *__restrict__ shots,
-                             int nshots, int nx_g, int nz, int pitch) {
+                             int nshots, int nx_g, int nz, int pitch, IllumNorm nm = IllumNorm()) {
     const long long n = (long long)nx_g * nz;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
          idx += (long long)gridDim.x * blockDim.x) {
@@ -97,10 +112,37 @@ static __global__ void stack_kernel(const float *__restrict__ sum, const float *
             const int i = x - shots[s].x0;
             if (i < 0 || i >= shots[s].nx) continue;
             const long long o = (shots[s].row_off + i) * pitch + j + COL_OFF;
-            acc += (double)sum[o] - (double)comp[o];
+            acc += normalise((double)sum[o] - (double)comp[o], nm, o, s);
         }
         stack[idx] = acc;
     }
+}
+
+// Source illumination of one snapshot component: for every cell of shot
+// blockIdx.y, I = sum over the imaging slots of snapshot^2 in FP64 (slot
+// order), written at the image index; the shot's maximum goes to imax[shot]
+// (atomicMax on the bits of a non-negative double).  Snapshot layout of the
+// forward: per shot [nsnap][nx][pitch] at nsnap * row_off * pitch.
+static __global__ void illum_kernel(const float *__restrict__ snap, const int *__restrict__ slots, int nslots,
+                                    int nsnap, const ShotDev *__restrict__ shots, int nz, int pitch,
+                                    double *__restrict__ illum, unsigned long long *__restrict__ imax) {
+    const ShotDev sh = shots[blockIdx.y];
+    const long long n = (long long)sh.nx * nz;
+    const float *base = snap + (long long)nsnap * sh.row_off * pitch;
+    double m = 0.0;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx / nz), j = (int)(idx % nz);
+        double acc = 0.0;
+        for (int k = 0; k < nslots; ++k) {
+            const double v = base[((long long)slots[k] * sh.nx + i) * pitch + j + COL_OFF];
+            acc += v * v;
+        }
+        illum[(sh.row_off + i) * pitch + j + COL_OFF] = acc;
+        m = fmax(m, acc);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(imax + blockIdx.y, (unsigned long long)__double_as_longlong(m));
 }
 
 }  // namespace rtm

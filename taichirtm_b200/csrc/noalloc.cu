@@ -139,7 +139,7 @@ Layout layout_for(const rtm_grid &g, int nsrc, int nrec, int n_work) {
     L.src_ent = take(sizeof(int2) * (size_t)(nsrc > 0 ? nsrc : 1));
     L.rec_ent = take(sizeof(int2) * (size_t)(nrec > 0 ? nrec : 1));
     L.seis_t = take(sizeof(float) * (size_t)3 * g.nt * (nrec > 0 ? nrec : 1));
-    L.flags = take(sizeof(int));
+    L.flags = take(2 * sizeof(int));  // status flag, then the first failing launch
     L.total = off;
     return L;
 }
@@ -254,6 +254,7 @@ int rtm_forward_noalloc(const rtm_grid *grid, int nsrc, const int32_t *src_ij, i
         if (L.mat[m] != SIZE_MAX) NA_TRY(cudaMemsetAsync(base + L.mat[m], 0, grid_f, s));
     NA_TRY(cudaMemsetAsync(base + L.seis_t, 0, sizeof(float) * (size_t)3 * g.nt * (nrec > 0 ? nrec : 1), s));
     NA_TRY(cudaMemsetAsync(base + L.flags, 0, sizeof(int), s));
+    NA_TRY(cudaMemsetAsync(base + L.flags + sizeof(int), 0x7f, sizeof(int), s));  // no failing launch yet
 
     const long long n = (long long)g.nx * g.nz;
     const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
@@ -286,6 +287,7 @@ int rtm_forward_noalloc(const rtm_grid *grid, int nsrc, const int32_t *src_ij, i
     sp.rec_ent = reinterpret_cast<const int2 *>(base + L.rec_ent);
     sp.nrec_total = nrec;
     sp.flags = reinterpret_cast<int *>(base + L.flags);
+    sp.fail_seq = reinterpret_cast<int *>(base + L.flags) + 1;
     sp.code_base = 1;
     sp.snap_k = -1;
     float *seis_t = F(L.seis_t);
@@ -300,6 +302,7 @@ int rtm_forward_noalloc(const rtm_grid *grid, int nsrc, const int32_t *src_ij, i
             sp.sout[f] = F(L.state[(it + 1) & 1][f]);
         }
         sp.it = it;
+        sp.seq = it + 1;
         sp.check = check_interval > 0 && it % check_interval == 0;
         NA_TRY(na_launch_mode(sp, g.modes, s));
     }

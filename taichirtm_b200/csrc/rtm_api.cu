@@ -80,6 +80,7 @@ struct rtm_plan {
     float *d_img[3] = {}, *d_imgc[3] = {};
     float *d_seis_t = nullptr, *d_obs_t = nullptr;
     int *d_flags = nullptr;
+    int *d_fail_seq = nullptr;  // per shot: first failing launch of the current loop
     bool model_set = false;
     long long launches = 0;
     // CUDA-graph replay of time loops (tune.graphs): one cached executable per
@@ -109,7 +110,7 @@ void plan_free(rtm_plan *p) {
     for (int m = 0; m < NMAT; ++m) F(p->d_mat[m]);
     F(p->d_surface); F(p->d_sponge);
     for (int c = 0; c < 3; ++c) { F(p->d_img[c]); F(p->d_imgc[c]); }
-    F(p->d_seis_t); F(p->d_obs_t); F(p->d_flags);
+    F(p->d_seis_t); F(p->d_obs_t); F(p->d_flags); F(p->d_fail_seq);
     for (auto *gc : {&p->g_fwd, &p->g_bwd, &p->g_ckpt})
         if (gc->exec) cudaGraphExecDestroy(gc->exec);
     if (p->ev_in) cudaEventDestroy(p->ev_in);
@@ -270,6 +271,7 @@ void fill_common(const rtm_plan *p, StepParams &sp) {
     sp.rec_ent = p->d_rec_ent;
     sp.nrec_total = p->nrec_total;
     sp.flags = p->d_flags;
+    sp.fail_seq = p->d_fail_seq;
     sp.snap_k = -1;
 }
 
@@ -279,6 +281,7 @@ int zero_state(rtm_plan *p, cudaStream_t s) {
             if (p->d_state[b][f])
                 CUDA_TRY(cudaMemsetAsync(p->d_state[b][f], 0, p->state_floats * sizeof(float), s));
     CUDA_TRY(cudaMemsetAsync(p->d_flags, 0, p->nshots * sizeof(int), s));
+    CUDA_TRY(cudaMemsetAsync(p->d_fail_seq, 0x7f, p->nshots * sizeof(int), s));  // 0x7f7f7f7f: none
     return 0;
 }
 
@@ -417,6 +420,7 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
     rc |= dalloc(&p->d_src_ent, std::max<size_t>(src_ent.size(), 1));
     rc |= dalloc(&p->d_rec_ent, std::max<size_t>(rec_ent.size(), 1));
     rc |= dalloc(&p->d_flags, nshots);
+    rc |= dalloc(&p->d_fail_seq, nshots);
     rc |= dalloc(&p->d_sponge, std::max(g.absorbing_frame, 1));
     for (int b = 0; b < 2 && !rc; ++b)
         for (int f = 0; f < NFIELD && !rc; ++f)
@@ -571,6 +575,7 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
                 sp.sout[f] = p->d_state[(L + 1) & 1][f];
             }
             sp.it = it;
+            sp.seq = it + 1;
             sp.snap_k = snap_at(it);
             if (sched[L].two) {
                 sp.it2 = it + 1;
@@ -605,9 +610,12 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
     return RTM_OK;
 }
 
-int rtm_backward(rtm_plan *p, const float *obs, const float *snap_u, const float *snap_v,
-                 const float *snap_w, const int32_t *isnaps, int num_snaps, int isnap, float *image,
-                 double *stack, int check_interval, int32_t *flags, rtm_stream_t stream) {
+// rtm_backward; norm_eps >= 0 adds the source-illumination normalisation of
+// rtm_backward_normalized.
+static int backward_impl(rtm_plan *p, const float *obs, const float *snap_u, const float *snap_v,
+                         const float *snap_w, const int32_t *isnaps, int num_snaps, int isnap, float *image,
+                         double *stack, int check_interval, int32_t *flags, rtm_stream_t stream,
+                         double norm_eps) {
     if (!p) return fail(RTM_E_ARG, "null plan");
     if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
     if (p->nrec_total > 0 && !obs) return fail(RTM_E_ARG, "null observed data");
@@ -662,6 +670,7 @@ int rtm_backward(rtm_plan *p, const float *obs, const float *snap_u, const float
                 sp.sout[f] = p->d_state[(L + 1) & 1][f];
             }
             sp.it = (nt - 1) - it;  // backward_modeling.py:549
+            sp.seq = it + 1;
             sp.snap_k = snap_of[it];
             if (sched[L].two) {
                 sp.it2 = (nt - 1) - (it + 1);
@@ -682,35 +691,80 @@ int rtm_backward(rtm_plan *p, const float *obs, const float *snap_u, const float
     if (int rc = run_loop(p, p->g_bwd, key, s, loop)) return rc;
     p->launches += (long long)sched.size();
     const int blocks = 148 * 8;
-    if (image) {
-        const size_t n = (size_t)p->g.nx * p->g.nz;
-        for (int c = 0; c < 3; ++c) {
+    const size_t n = (size_t)p->g.nx * p->g.nz;
+    // source illumination (rtm_backward_normalized): FP64 per cell, one
+    // component at a time, over the snapshot slots the correlation used
+    struct Scratch {
+        double *illum = nullptr;
+        unsigned long long *imax = nullptr;
+        int *slots = nullptr;
+        ~Scratch() {
+            if (illum) cudaFree(illum);
+            if (imax) cudaFree(imax);
+            if (slots) cudaFree(slots);
+        }
+    } sc;
+    std::vector<int> slots;
+    const bool norm = norm_eps >= 0.0;
+    if (norm) {
+        for (int it = 0; it < nt; ++it)
+            if (snap_of[it] >= 0) slots.push_back(snap_of[it]);
+        if (int rc = dalloc(&sc.illum, img_floats)) return rc;
+        if (int rc = dalloc(&sc.imax, (size_t)p->nshots)) return rc;
+        if (!slots.empty()) {
+            if (int rc = dalloc(&sc.slots, slots.size())) return rc;
+            CUDA_TRY(cudaMemcpyAsync(sc.slots, slots.data(), slots.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+        }
+    }
+    for (int c = 0; c < 3; ++c) {
+        IllumNorm nm;
+        if (norm && p->d_img[c]) {
+            CUDA_TRY(cudaMemsetAsync(sc.imax, 0, (size_t)p->nshots * sizeof(unsigned long long), s));
+            illum_kernel<<<dim3(64, p->nshots), 256, 0, s>>>(sp3[c], sc.slots, (int)slots.size(), num_snaps,
+                                                             p->d_shots, p->g.nz, p->pitch, sc.illum, sc.imax);
+            CUDA_TRY(cudaGetLastError());
+            ++p->launches;
+            nm.illum = sc.illum;
+            nm.imax = sc.imax;
+            nm.eps = norm_eps;
+        }
+        if (image) {
             float *dst = image + c * n;
             if (p->d_img[c]) {
-                image_out_kernel<<<blocks, 256, 0, s>>>(p->d_img[c], p->d_imgc[c], dst, 0,
-                                                        p->shots_h[0].nx, p->g.nz, p->pitch);
+                image_out_kernel<<<blocks, 256, 0, s>>>(p->d_img[c], p->d_imgc[c], dst, 0, p->shots_h[0].nx,
+                                                        p->g.nz, p->pitch, nm);
                 CUDA_TRY(cudaGetLastError());
                 ++p->launches;
             } else {
                 CUDA_TRY(cudaMemsetAsync(dst, 0, n * sizeof(float), s));
             }
         }
+        if (stack && p->d_img[c]) {
+            stack_kernel<<<blocks, 256, 0, s>>>(p->d_img[c], p->d_imgc[c], stack + c * n, p->d_shots, p->nshots,
+                                                p->g.nx, p->g.nz, p->pitch, nm);
+            CUDA_TRY(cudaGetLastError());
+            ++p->launches;
+        }
     }
-    if (stack) {
-        const size_t n = (size_t)p->g.nx * p->g.nz;
-        for (int c = 0; c < 3; ++c)
-            if (p->d_img[c]) {
-                stack_kernel<<<blocks, 256, 0, s>>>(p->d_img[c], p->d_imgc[c], stack + c * n, p->d_shots,
-                                                    p->nshots, p->g.nx, p->g.nz, p->pitch);
-                CUDA_TRY(cudaGetLastError());
-                ++p->launches;
-            }
-    }
-    if (flags) {
-        CUDA_TRY(cudaMemcpyAsync(flags, p->d_flags, p->nshots * sizeof(int), cudaMemcpyDeviceToHost, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
-    }
+    if (flags) CUDA_TRY(cudaMemcpyAsync(flags, p->d_flags, p->nshots * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (flags || norm) CUDA_TRY(cudaStreamSynchronize(s));  // scratch is freed on return
     return RTM_OK;
+}
+
+int rtm_backward(rtm_plan *p, const float *obs, const float *snap_u, const float *snap_v,
+                 const float *snap_w, const int32_t *isnaps, int num_snaps, int isnap, float *image,
+                 double *stack, int check_interval, int32_t *flags, rtm_stream_t stream) {
+    return backward_impl(p, obs, snap_u, snap_v, snap_w, isnaps, num_snaps, isnap, image, stack, check_interval,
+                         flags, stream, -1.0);
+}
+
+int rtm_backward_normalized(rtm_plan *p, const float *obs, const float *snap_u, const float *snap_v,
+                            const float *snap_w, const int32_t *isnaps, int num_snaps, int isnap, float eps,
+                            float *image, double *stack, int check_interval, int32_t *flags,
+                            rtm_stream_t stream) {
+    if (!(eps >= 0.0f) || !std::isfinite(eps)) return fail(RTM_E_ARG, "eps must be finite and >= 0");
+    return backward_impl(p, obs, snap_u, snap_v, snap_w, isnaps, num_snaps, isnap, image, stack, check_interval,
+                         flags, stream, (double)eps);
 }
 
 size_t rtm_plan_state_floats(const rtm_plan *p) { return p ? p->state_floats : 0; }
@@ -847,6 +901,7 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
             sp.sout[f] = out[f];
         }
         sp.it = ln.it;
+        sp.seq = ln.it + 1;
         sp.check = check_at(last);
         if (ln.two) {
             sp.it2 = last;
@@ -897,7 +952,7 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
     const size_t nrec_slots = (size_t)std::max(K - 1, 1);
     const size_t nslots = nrec_slots + 1 + 2 + (ckpt_dtype == RTM_CKPT_F32 ? 0 : 1);
     int rc = dalloc(&seg, nslots * slot);
-    if (!rc) rc = dalloc(&gsum, (size_t)2 * NGRAD * gfl);
+    if (!rc) rc = dalloc(&gsum, (size_t)3 * NGRAD * gfl);  // Kahan sums, compensations, partials
     if (!rc && grad_wavelet && p->nsrc_total) rc = dalloc(&gwt, (size_t)3 * nt * p->nsrc_total);
     auto cleanup = [&]() {
         if (seg) cudaFree(seg);
@@ -910,8 +965,9 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
     }
     auto body = [&]() -> int {
         CUDA_TRY(cudaMemsetAsync(p->d_flags, 0, p->nshots * sizeof(int), s));
+        CUDA_TRY(cudaMemsetAsync(p->d_fail_seq, 0x7f, p->nshots * sizeof(int), s));
         CUDA_TRY(cudaMemsetAsync(seg, 0, nslots * slot * sizeof(float), s));
-        CUDA_TRY(cudaMemsetAsync(gsum, 0, (size_t)2 * NGRAD * gfl * sizeof(float), s));
+        CUDA_TRY(cudaMemsetAsync(gsum, 0, (size_t)3 * NGRAD * gfl * sizeof(float), s));
         if (gwt) CUDA_TRY(cudaMemsetAsync(gwt, 0, (size_t)3 * nt * p->nsrc_total * sizeof(float), s));
         if (p->nrec_total) {
             if (int r = transpose(resid, p->d_obs_t, 3, p->nrec_total, nt, s)) return r;
@@ -962,9 +1018,13 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
             ap.resid[c] = p->d_obs_t + c * plane;
             ap.gwav[c] = gwt ? gwt + (size_t)c * nt * p->nsrc_total : nullptr;
         }
+        GradFold fold;
+        fold.n = (long long)gfl;
         for (int g = 0; g < NGRAD; ++g) {
-            ap.grad[g] = gsum + (size_t)g * gfl;
-            ap.gradc[g] = gsum + (size_t)(NGRAD + g) * gfl;
+            fold.sum[g] = gsum + (size_t)g * gfl;
+            fold.comp[g] = gsum + (size_t)(NGRAD + g) * gfl;
+            fold.part[g] = gsum + (size_t)(2 * NGRAD + g) * gfl;
+            ap.gpart[g] = fold.part[g];
         }
         int cur = 0;
         const int warps = p->warps;
@@ -983,6 +1043,7 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
                     sp.sout[f] = fld(dst, f);
                 }
                 sp.it = it;
+                sp.seq = it + 1;
                 CUDA_TRY((launch_mode<0>(sp, RTM_PSV, p->vec | (p->prefetch << 8), warps, s)));
                 ++p->launches;
             }
@@ -1003,11 +1064,16 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
                 CUDA_TRY(cudaGetLastError());
                 ++p->launches;
                 cur = 1 - cur;
+                if (n % GRAD_FOLD_STEPS == 0) {  // n = 0 is the last step: everything is folded
+                    grad_fold_kernel<<<148 * 8, 256, 0, s>>>(fold);
+                    CUDA_TRY(cudaGetLastError());
+                    ++p->launches;
+                }
             }
         }
         const size_t n2 = (size_t)p->g.nx * p->g.nz;
         for (int g = 0; g < NGRAD; ++g) {
-            stack_kernel<<<148 * 8, 256, 0, s>>>(ap.grad[g], ap.gradc[g], grad + g * n2, p->d_shots, p->nshots,
+            stack_kernel<<<148 * 8, 256, 0, s>>>(fold.sum[g], fold.comp[g], grad + g * n2, p->d_shots, p->nshots,
                                                  p->g.nx, p->g.nz, p->pitch);
             CUDA_TRY(cudaGetLastError());
         }
@@ -1107,6 +1173,7 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
                     fp.sout[f] = dst + (size_t)f * sf;
                 }
                 fp.it = it;
+                fp.seq = it + 1;
                 fp.snap_k = slot_at(it);
                 if (fsched[L].two) {
                     fp.it2 = it + 1;
@@ -1127,6 +1194,7 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
                     bp.sout[f] = p->d_state[(nb + 1) & 1][f];
                 }
                 bp.it = t;
+                bp.seq = it + 1;
                 bp.snap_k = slot_at(t);
                 if (ln.two) {
                     bp.it2 = t - 1;

@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     const int task = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (task >= p.n_work) return;
     const int4 wk = p.work[task];
-    if (__ldg(p.flags + wk.x) != 0) return;  // this shot already failed: stop it
+    if (shot_stopped(p, wk.x)) return;
     const ShotDev sh = p.shots[wk.x];
     const int nx = sh.nx, nz = p.nz, P = p.pitch;
     const int j0 = (wk.y & 0xFFFFF) * W;
@@ -528,7 +528,7 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     }
     if (p.check) {
         code = __reduce_max_sync(FULL, code);
-        if (lane == 0 && code > 0) atomicMax(p.flags + wk.x, code);
+        if (lane == 0 && code > 0) report_failure(p, wk.x, code);
     }
 }
 

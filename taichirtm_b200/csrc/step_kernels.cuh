@@ -83,6 +83,8 @@ struct StepParams {
     int check;               // run the finite check this step
     int code_base;           // 1 forward, 4 backward
     int *flags;              // per shot status
+    int *fail_seq;           // per shot: seq of the launch whose check first failed (INT_MAX: none)
+    int seq;                 // this launch's number in its time loop (increasing)
     int it;                  // forward: step it; backward: reversed time t
     int it2, snap_k2;        // two-step launches: time and snapshot slot of the second step
 };
@@ -195,6 +197,21 @@ __device__ __forceinline__ bool interior(int i, int j, int nx, int nz) {
     return (unsigned)(i - 1) < (unsigned)(nx - 2) && (unsigned)(j - 1) < (unsigned)(nz - 2);
 }
 
+// A shot whose finite check failed in an EARLIER launch is stopped.  Warps of
+// the failing launch itself all finish, whatever order they run in, so every
+// row is updated, recorded and imaged at the failing step, as the reference
+// does before it returns (forward_modeling.py:562-566).
+__device__ __forceinline__ bool shot_stopped(const StepParams &p, int shot) {
+    return p.fail_seq ? p.fail_seq[shot] < p.seq : __ldg(p.flags + shot) != 0;
+}
+
+// Record a failed check of this launch: the highest code wins, the first
+// failing launch stops the shot for the launches after it.
+__device__ __forceinline__ void report_failure(const StepParams &p, int shot, int code) {
+    atomicMax(p.flags + shot, code);
+    if (p.fail_seq) atomicMin(p.fail_seq + shot, p.seq);
+}
+
 __device__ __forceinline__ int bad_code(float x, int code) {
     return (isnan(x) || fabsf(x) > 1e30f) ? code : 0;
 }
@@ -242,7 +259,7 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
     const int task = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (task >= p.n_work) return;
     const int4 wk = p.work[task];
-    if (__ldg(p.flags + wk.x) != 0) return;  // this shot already failed: stop it
+    if (shot_stopped(p, wk.x)) return;
     const ShotDev sh = p.shots[wk.x];
     const int nx = sh.nx, nz = p.nz, P = p.pitch;
     // wk.y: strip in bits 0-19; bit 20 / 21 set = no source / no receiver in
@@ -767,7 +784,7 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
     }
     if (p.check) {
         code = __reduce_max_sync(FULL, code);
-        if (lane == 0 && code > 0) atomicMax(p.flags + wk.x, code);
+        if (lane == 0 && code > 0) report_failure(p, wk.x, code);
     }
 }
 

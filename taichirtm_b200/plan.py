@@ -123,9 +123,11 @@ class Plan:
         return flags, seis, (snaps if save else None), isnaps[:nsnap]
 
     def backward(self, obs, snaps, isnaps, num_snaps, isnap, check_interval=100, image=True,
-                 stack=None, stream=None):
+                 stack=None, stream=None, normalize_eps=None):
         """obs: (3, nrec_total, nt).  Returns (flags, image (3, nx, nz) or None,
-        stack (3, nx, nz) float64 or None)."""
+        stack (3, nx, nz) float64 or None).  normalize_eps (>= 0) selects the
+        source-normalised cross-correlation: every shot's image divided by its
+        source illumination + eps * its maximum (rtm_backward_normalized)."""
         o = self._f32(obs, (3, self.nrec_total, self.nt)) if self.nrec_total else None
         isn = np.ascontiguousarray(np.asarray(isnaps, np.int32).reshape(-1))
         if isn.size == 0:
@@ -134,10 +136,16 @@ class Plan:
         flags = np.zeros(len(self.shots), np.int32)
         snaps = snaps if snaps is not None else [None, None, None]
         with torch.cuda.device(self.device):
-            check(_lib.lib().rtm_backward(self.h, _ptr(o), _ptr(snaps[0]), _ptr(snaps[1]),
-                                          _ptr(snaps[2]), _i32p(isn), int(num_snaps), int(isnap),
-                                          _ptr(img), _ptr(stack), int(check_interval), _i32p(flags),
-                                          _stream(stream)), "rtm_backward")
+            if normalize_eps is None:
+                check(_lib.lib().rtm_backward(self.h, _ptr(o), _ptr(snaps[0]), _ptr(snaps[1]),
+                                              _ptr(snaps[2]), _i32p(isn), int(num_snaps), int(isnap),
+                                              _ptr(img), _ptr(stack), int(check_interval), _i32p(flags),
+                                              _stream(stream)), "rtm_backward")
+            else:
+                check(_lib.lib().rtm_backward_normalized(
+                    self.h, _ptr(o), _ptr(snaps[0]), _ptr(snaps[1]), _ptr(snaps[2]), _i32p(isn), int(num_snaps),
+                    int(isnap), float(normalize_eps), _ptr(img), _ptr(stack), int(check_interval), _i32p(flags),
+                    _stream(stream)), "rtm_backward_normalized")
         return flags, img, stack
 
     def _comp_active(self, c):

@@ -46,9 +46,14 @@ def test_reference_names_exported():
     sig = inspect.signature(T.ForwardModeling.run)
     assert list(sig.parameters)[1:] == ["save", "display_callback", "stability_check_interval"]
     sig = inspect.signature(T.BackwardModeling.run_calc)
-    assert list(sig.parameters)[1:] == ["import_fwdata_u", "import_fwdata_v", "import_fwdata_w",
-                                        "isnaps_field", "num_snaps", "isnap_interval", "method",
-                                        "display_callback", "stability_check_interval"]
+    ref = ["import_fwdata_u", "import_fwdata_v", "import_fwdata_w", "isnaps_field", "num_snaps",
+           "isnap_interval", "method", "display_callback", "stability_check_interval"]
+    names = list(sig.parameters)[1:]
+    assert names[:len(ref)] == ref
+    # extensions only as keyword-only parameters with defaults after the reference's
+    for n in names[len(ref):]:
+        prm = sig.parameters[n]
+        assert prm.kind is inspect.Parameter.KEYWORD_ONLY and prm.default is not inspect.Parameter.empty, n
 
 
 def test_product_has_no_oracle_dependency():

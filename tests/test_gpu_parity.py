@@ -250,3 +250,46 @@ def test_reverse_time_migration_run_golden(name):
         if np.abs(g["img"][k]).max() > 0:
             assert rel_l2(img[k], g["img"][k]) <= IMG_TOL, (k, rel_l2(img[k], g["img"][k]))
     r.cleanup()
+
+
+def test_source_normalized_imaging_vs_fp64_oracle():
+    """method="source_normalized" (extension): the cross-correlation image of
+    each component divided by the source illumination sum_t snapshot^2 +
+    eps * max, against the FP64 oracle; rel-L2 <= 1e-4.  The same through
+    BatchedRTM.migrate's FP64 stack."""
+    from oracle import fd_oracle
+    from taichirtm_b200 import BackwardModeling, ForwardModeling
+    from taichirtm_b200.batch import BatchedRTM
+    from taichirtm_b200.plan import ShotGeometry
+    g = load_golden("fwbw_basic")
+    c = _common(g)
+    c.pop("surface_matrix_field")
+    wav = dict(wavelet_u_field=g["wu"], wavelet_v_field=g["wv"], wavelet_w_field=g["ww"])
+    isnap, eps = 3, 1e-3
+    fm = ForwardModeling(isnap=isnap, **_fields(g, "s"), **c, **wav)
+    assert fm.run(save=True) == 0
+    bw = BackwardModeling(obsdata_u_field=g["obs"][0], obsdata_v_field=g["obs"][1], obsdata_w_field=g["obs"][2],
+                          **_fields(g, "s"), **c)
+    assert bw.run_calc(fm.u_save_field, fm.v_save_field, fm.w_save_field, fm.isnaps_field, fm.num_snaps, isnap,
+                       method="source_normalized", normalization_eps=eps) == 0
+    img = np.stack(bw.get_results())
+    kw = dict(dx=float(g["dx"]), dz=float(g["dz"]), nt=int(g["nt"]), fs=float(g["fs"]), fw=int(g["fw"]))
+    f = fd_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], src=g["src"], wu=g["wu"], wv=g["wv"], ww=g["ww"],
+                          rec=g["rec"], isnap=isnap, save=True, **kw)
+    b = fd_oracle.backward(g["mu_s"], g["lam_s"], g["rho_s"], rec=g["rec"], ou=g["obs"][0], ov=g["obs"][1],
+                           ow=g["obs"][2], snaps=f["snaps"], isnaps=f["isnaps"], num_snaps=f["num_snaps"],
+                           isnap=isnap, **kw)
+    slots = fd_oracle.imaging_slots(kw["nt"], isnap, f["isnaps"], f["num_snaps"])
+    ref = fd_oracle.source_normalized(b["img"], f["snaps"], slots, eps)
+    assert np.abs(ref).max() > 0
+    e = rel_l2(img, ref)
+    assert e <= IMG_TOL, e
+    assert rel_l2(img, b["img"]) > 0.5  # the plain correlation is a different image
+    # batched path: the FP64 stack of one full-window shot
+    b2 = BatchedRTM(g["mu_s"], g["lam_s"], g["rho_s"], kw["dx"], kw["dz"], kw["fs"], kw["nt"], kw["fw"],
+                    [ShotGeometry(0, c["nx"], g["src"], g["rec"])], modes=3, tune=None)
+    w = np.stack([g["wu"], g["wv"], g["ww"]])
+    _, _, st = b2.migrate(w, g["obs"], isnap=isnap, method="source_normalized", normalization_eps=eps)
+    e2 = rel_l2(st.cpu().numpy(), ref)
+    assert e2 <= IMG_TOL, e2
+    b2.close()

@@ -75,13 +75,14 @@ def _run(C, modes, tune, isnap, check=7, surface=None):
 
 
 def _same(a, b):
+    """Bit-identical outputs; NaN (after a failed check) compares equal to NaN."""
     assert np.array_equal(a["ff"], b["ff"]) and np.array_equal(a["fb"], b["fb"])
-    assert np.array_equal(a["seis"], b["seis"])
-    assert np.array_equal(a["img"], b["img"])
+    assert np.array_equal(a["seis"], b["seis"], equal_nan=True)
+    assert np.array_equal(a["img"], b["img"], equal_nan=True)
     for x, y in zip(a["snaps"], b["snaps"]):
         assert (x is None) == (y is None)
         if x is not None:
-            assert np.array_equal(x, y)
+            assert np.array_equal(x, y, equal_nan=True)
 
 
 @pytest.mark.parametrize("modes", [1, 2, 3])
@@ -172,3 +173,40 @@ def test_two_steps_fwi_gradient_bit_identical():
         grads.append((seis.cpu().numpy(), g[0].cpu().numpy() if isinstance(g, tuple) else g.cpu().numpy()))
     assert np.array_equal(grads[0][0], grads[1][0])
     assert np.array_equal(grads[0][1], grads[1][1])
+
+
+def test_failing_check_step_is_complete_for_every_launch_shape():
+    """A huge wavelet sample at step 7 overflows the check threshold; the check
+    at step 10 (interval 5) fails.  The reference records step 10 in full and
+    then returns (forward_modeling.py:550-566), so every warp of the failing
+    launch must finish its rows: the seismograms, up to and including step
+    10, are bit-identical for every launch shape (one and two steps per
+    launch, different warps per CTA) and to the NumPy FP32 restatement, which
+    stops at the same check; later samples stay zero."""
+    from oracle import fd_oracle
+    from taichirtm_b200.plan import Plan, ShotGeometry
+    C = _case(nx=64, nz=70, nt=24, fw=8)
+    src = np.array([[32, 6]], np.int32)  # the step-2 pulse reaches the j = 1 receivers by step 10
+    wav = np.zeros((3, 1, C["nt"]), np.float32)
+    wav[2, 0, 2] = 1.0
+    wav[2, 0, 7] = 1e36
+    mu, lam, rho = C["model"]
+    kw = dict(dx=C["dx"], dz=C["dz"], nt=C["nt"], fs=C["fs"], fw=C["fw"])
+    ref = fd_oracle.forward(mu, lam, rho, src=src, wu=wav[0, 0], wv=wav[1, 0], ww=wav[2, 0], rec=C["rec"],
+                            check_interval=5, dtype=np.float32, setup_f64=True, **kw)
+    assert ref["flag"] in (1, 3)
+    outs = []
+    for tune in (dict(vec=2, rows=4, warps=2, tsteps=1), dict(vec=2, rows=4, warps=2, tsteps=2),
+                 dict(vec=1, rows=3, warps=1, prefetch=0), dict(vec=4, rows=64, warps=8, prefetch=3),
+                 dict(vec=4, rows=2, warps=8, tsteps=2)):
+        p = Plan(C["nx"], C["nz"], C["dx"], C["dz"], C["nt"], C["fs"], C["fw"], 1,
+                 [ShotGeometry(0, C["nx"], src, C["rec"])], tune=tune)
+        p.set_model(mu, lam, rho)
+        f, seis, _, _ = p.forward(torch.as_tensor(wav), check_interval=5)
+        outs.append((int(f[0]), seis.cpu().numpy()))
+        p.close()
+    for code, seis in outs:
+        assert code == ref["flag"]
+        assert np.array_equal(seis[[0, 2]], ref["seis"][[0, 2]], equal_nan=True)
+        assert np.abs(seis[:, :, 11:]).max() == 0.0
+        assert np.nanmax(np.abs(seis[:, :, 10])) > 0.0

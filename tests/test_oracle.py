@@ -110,3 +110,24 @@ def test_modes_split_exact():
     sh = c_oracle.forward(g["mu_s"], g["lam_s"], g["rho_s"], modes=2, **kw)["seis"]
     assert np.array_equal(both[[0, 2]], psv[[0, 2]])
     assert np.array_equal(both[1], sh[1])
+
+
+def test_imaging_slots_and_source_normalization_definition():
+    """The imaging-step gate restated for the source-normalised condition
+    selects exactly the slots the golden backward runs correlate, and the
+    normalisation divides by sum snapshot^2 + eps * max (0 where that is 0)."""
+    g = load_golden("fwbw_basic")
+    nt, isnap, ns = int(g["nt"]), int(g["isnap"]), int(g["num_snaps"])
+    slots = fd_oracle.imaging_slots(nt, isnap, g["isnaps"], ns)
+    ts = [(nt - 1) - it for it in range(nt)]
+    want = [t // isnap - 1 for t in ts if t > 0 and t % isnap == 0 and t // isnap - 1 < ns
+            and int(g["isnaps"][t // isnap - 1]) == t]
+    assert slots == want and len(slots) > 0
+    rng = np.random.default_rng(3)
+    snaps = rng.standard_normal((3, 5, 4, 6))
+    snaps[1] = 0.0
+    img = rng.standard_normal((3, 5, 4))
+    out = fd_oracle.source_normalized(img, snaps, [0, 2, 5], 0.1)
+    ill = (snaps[0][..., [0, 2, 5]] ** 2).sum(-1)
+    assert np.allclose(out[0], img[0] / (ill + 0.1 * ill.max()))
+    assert np.all(out[1] == 0.0)
