@@ -201,6 +201,16 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
         // ---- pointwise quantities of row k
         const Row cur = nxt;
         if (k < ib) load_row(k + 1, nxt, true);
+        // gradient partial sums of row k-1 (finished below): issued here so
+        // that their latency overlaps the arithmetic of row k (at VEC 4 the
+        // registers are not there: loaded where they are used)
+        constexpr bool HOIST = VEC <= 2;
+        float gp[NGRAD][VEC];
+        const long long go = (sh.row_off + (k - 1)) * (long long)P + c0 + COL_OFF;
+        if (HOIST && k >= ia + 1 && owner) {
+#pragma unroll
+            for (int gi = 0; gi < NGRAD; ++gi) ldv<VEC>(gp[gi], p.gpart[gi] + go);
+        }
         float sxx[VEC], szz[VEC], sxz[VEC], bxx[VEC], bzz[VEC], bxz[VEC];
         float lam[VEC], mu[VEC], mxz[VEC], sm[VEC];
 #pragma unroll
@@ -357,12 +367,11 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
                 stv<VEC>(p.aout[A_SXX] + so, oxx);
                 stv<VEC>(p.aout[A_SZZ] + so, ozz);
                 stv<VEC>(p.aout[A_SXZ] + so, oxz);
-                const long long go = (sh.row_off + r) * (long long)P + c0 + COL_OFF;
                 auto acc = [&](int gi, const float (&d)[VEC]) {
                     float s[VEC];
-                    ldv<VEC>(s, p.gpart[gi] + go);
+                    if constexpr (!HOIST) ldv<VEC>(gp[gi], p.gpart[gi] + go);
 #pragma unroll
-                    for (int q = 0; q < VEC; ++q) s[q] = __fadd_rn(s[q], d[q]);
+                    for (int q = 0; q < VEC; ++q) s[q] = __fadd_rn(gp[gi][q], d[q]);
                     stv<VEC>(p.gpart[gi] + go, s);
                 };
                 acc(G_LAM, dl);

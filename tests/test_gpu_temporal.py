@@ -192,8 +192,9 @@ def test_failing_check_step_is_complete_for_every_launch_shape():
     wav[2, 0, 7] = 1e36
     mu, lam, rho = C["model"]
     kw = dict(dx=C["dx"], dz=C["dz"], nt=C["nt"], fs=C["fs"], fw=C["fw"])
-    ref = fd_oracle.forward(mu, lam, rho, src=src, wu=wav[0, 0], wv=wav[1, 0], ww=wav[2, 0], rec=C["rec"],
-                            check_interval=5, dtype=np.float32, setup_f64=True, **kw)
+    with np.errstate(over="ignore", invalid="ignore"):  # the blow-up is the point
+        ref = fd_oracle.forward(mu, lam, rho, src=src, wu=wav[0, 0], wv=wav[1, 0], ww=wav[2, 0], rec=C["rec"],
+                                check_interval=5, dtype=np.float32, setup_f64=True, **kw)
     assert ref["flag"] in (1, 3)
     outs = []
     for tune in (dict(vec=2, rows=4, warps=2, tsteps=1), dict(vec=2, rows=4, warps=2, tsteps=2),
