@@ -342,6 +342,8 @@ def main():
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier(device_ids=[local])
     t_start.record(stream)
     for k in range(args.steps):
         ff, fb, n_launch = one_step(evs[k])
@@ -351,6 +353,8 @@ def main():
         stack = reduce_result(stack, status)  # cross-GPU image stack (FP64), after a status check
     t_end.record(stream)
     torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier(device_ids=[local])
     clocks = sampler.stop(os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0] or None)
     ms = t_start.elapsed_time(t_end)
     fwd_ms = sum(e[0].elapsed_time(e[1]) for e in evs)
