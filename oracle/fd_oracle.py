@@ -244,7 +244,7 @@ def forward(mu, lam, rho, dx, dz, nt, fs, fw, src, wu, wv, ww, rec, isnap=10,
     p = Propagator(mu, lam, rho, dx, dz, fs, fw, surface, dtype, setup_f64)
     src = np.asarray(src).reshape(-1, 2)
     rec = np.asarray(rec).reshape(-1, 2)
-    wu, wv, ww = (np.asarray(x, dtype).reshape(len(src), -1) for x in (wu, wv, ww))
+    wu, wv, ww = (np.asarray(x, dtype).reshape(len(src), nt) for x in (wu, wv, ww))  # nt: also for no source
     nrec = len(rec)
     seis = np.zeros((3, nrec, nt), dtype)
     snaps = isnaps = None
