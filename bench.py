@@ -417,8 +417,9 @@ def main():
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        ff, fb, st = rtm.migrate(wav_h.to(dev, non_blocking=True), obs_h.to(dev, non_blocking=True),
-                                 isnap=ISNAP, check_interval=100)
+        # observed data stay in pinned host memory: migrate copies them on a
+        # side stream while the forward pass runs (the backward reads them)
+        ff, fb, st = rtm.migrate(wav_h.to(dev, non_blocking=True), obs_h, isnap=ISNAP, check_interval=100)
         if world > 1:
             st = reduce_result(st, max(int(ff.max()), int(fb.max())))
         host_img = st.cpu()

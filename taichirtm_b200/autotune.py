@@ -104,3 +104,53 @@ def best_shape(make_plan, nz, shots, modes, nt, candidates=None, refresh=False):
     cache[k] = dict(tune=best, ms_per_step=ms, tried=[dict(t, ms=m) for m, t in results])
     _store(cache)
     return best
+
+
+# FWI gradients: the exact adjoint kernel dominates and prefers more, smaller
+# warp tasks than the forward step, so FWIProblem(tune="auto") times the
+# gradient itself (checkpointed forward + adjoint sweep) on a short time axis.
+FWI_CANDIDATES = [dict(vec=2, rows=r, warps=w, tsteps=2) for r in (4, 8, 16) for w in (1, 2, 4)]
+FWI_TUNE_STEPS = 160
+
+
+def time_fwi_shape(make_problem, nx, nz, tune, steps=FWI_TUNE_STEPS):
+    """ms per time step of one gradient (checkpointed forward + adjoint) on a
+    homogeneous model; kernel times do not depend on the values."""
+    prob = make_problem(tune, steps)
+    try:
+        dev = prob.device
+        rho = torch.full((nx, nz), 2200.0, dtype=torch.float32, device=dev)
+        mu = rho * 1400.0 ** 2
+        lam = rho * 2500.0 ** 2 - 2 * mu
+        seis, ck, _ = prob.forward(lam, mu, rho)
+        prob.adjoint(seis, ck)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        seis, ck, _ = prob.forward(lam, mu, rho)
+        prob.adjoint(seis, ck)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+    finally:
+        prob.close()
+
+
+def best_fwi_shape(make_problem, nx, nz, shots, candidates=None, refresh=False):
+    """Cached best launch shape for FWI gradients; tunes on a miss."""
+    k = "fwi|" + key(nz, shots, 1)
+    cache = _load()
+    if not refresh and k in cache:
+        return cache[k]["tune"]
+    results = []
+    for t in candidates or FWI_CANDIDATES:
+        try:
+            results.append((time_fwi_shape(make_problem, nx, nz, t), t))
+        except Exception:
+            continue
+    if not results:
+        return None
+    ms, best = min(results, key=lambda r: r[0])
+    cache[k] = dict(tune=best, ms_per_step=ms, tried=[dict(t, ms=m) for m, t in results])
+    _store(cache)
+    return best

@@ -17,6 +17,23 @@ from .fields import to_tensor
 from .plan import PSV, SH, Plan, ShotGeometry, _i32p, _ptr, _stream, check, require_cuda
 
 
+class _StreamedTensor:
+    """A device tensor being filled on a side stream: ``get()`` makes the
+    current stream wait for that copy, then returns the tensor."""
+
+    def __init__(self, t, stream):
+        self.t, self.event = t, torch.cuda.Event()
+        self.event.record(stream)
+
+    def get(self):
+        torch.cuda.current_stream(self.t.device).wait_event(self.event)
+        return self.t
+
+
+def _ready(x):
+    return x.get() if isinstance(x, _StreamedTensor) else x
+
+
 class BatchedRTM:
     """Many shots on one model.
 
@@ -83,9 +100,13 @@ class BatchedRTM:
 
         ``method="source_normalized"`` divides every shot's image by its source
         illumination (sum of squared snapshots over the imaging steps) plus
-        ``normalization_eps`` times its maximum before stacking (snapshot path)."""
+        ``normalization_eps`` times its maximum before stacking (snapshot path).
+
+        ``observed`` may be a pinned host float32 tensor: it is then copied
+        to the device on a side stream while the forward pass runs (only the
+        backward pass reads it)."""
         w = to_tensor(wavelets, torch.float32, self.device)
-        o = to_tensor(observed, torch.float32, self.device)
+        o = self._observed_async(observed)
         if checkpoint:
             if method == "source_normalized":
                 raise ValueError("source_normalized imaging needs the snapshot path (checkpoint=None)")
@@ -93,11 +114,30 @@ class BatchedRTM:
         ff, _, snaps, isnaps = self.plan.forward(w, save=True, isnap=isnap, check_interval=check_interval)
         if stack is None:
             stack = torch.zeros((3, self.nx, self.nz), dtype=torch.float64, device=self.device)
+        o = _ready(o)
         fb, _, _ = self.plan.backward(o, snaps, isnaps, len(isnaps), isnap, check_interval=check_interval,
                                       image=False, stack=stack,
                                       normalize_eps=normalization_eps if method == "source_normalized" else None)
         del snaps
         return ff, fb, stack
+
+    def _observed_async(self, observed):
+        """Device copy of ``observed``; a pinned contiguous float32 host tensor
+        goes over on a side stream, and the current stream waits for it only
+        when the copy is first used, i.e. before the backward pass."""
+        if not (isinstance(observed, torch.Tensor) and observed.device.type == "cpu" and observed.is_pinned()
+                and observed.dtype == torch.float32 and observed.is_contiguous()):
+            return to_tensor(observed, torch.float32, self.device)
+        main = torch.cuda.current_stream(self.device)
+        side = getattr(self, "_copy_stream", None)
+        if side is None:
+            side = self._copy_stream = torch.cuda.Stream(device=self.device)
+        side.wait_stream(main)  # the destination's previous users are done
+        with torch.cuda.stream(side):
+            dst = torch.empty(observed.shape, dtype=torch.float32, device=self.device)
+            dst.copy_(observed, non_blocking=True)
+        dst.record_stream(main)
+        return _StreamedTensor(dst, side)
 
     def checkpoint_bytes(self, every, dtype="f32"):
         return int(_lib.lib().rtm_plan_checkpoint_bytes(self.plan.h, int(every), _lib.CKPT_DTYPES[dtype]))
@@ -116,6 +156,7 @@ class BatchedRTM:
         with torch.cuda.device(self.device):
             check(L.rtm_forward_checkpointed(self.plan.h, _ptr(w), _ptr(seis), every, dt, _ptr(ck),
                                              int(check_interval), _i32p(ff), _stream()), "rtm_forward_checkpointed")
+            o = _ready(o)
             check(L.rtm_backward_checkpointed(self.plan.h, _ptr(w), _ptr(o), every, dt, _ptr(ck), int(isnap), None,
                                               _ptr(stack), int(check_interval), _i32p(fb), _stream()),
                   "rtm_backward_checkpointed")

@@ -53,7 +53,7 @@ def run_c4(args):
     true.close()
     K = max(1, round(math.sqrt(nt)))
     prob = FWIProblem(sv.nx, sv.nz, sv.dx, sv.dz, sv.fs, nt, sv.fw, shots, wav, ckpt_every=K,
-                      tune={k: v for k, v in tune.items() if k != "graphs"}, device=dev)
+                      tune="auto", device=dev)
     m0 = [torch.tensor(x, dtype=torch.float64, device=dev) for x in (sv.vp_mig, sv.vs_mig, sv.rho_mig)]
 
     def gradient():
@@ -91,7 +91,7 @@ def run_c4(args):
                 data="synthetic", config=dict(workload="c4 FWI gradient: 8 shots, 1201x401, dx=5 m, dt=0.5 ms, "
                                                         f"nt={nt}, L2 misfit on vx and vz, start = smoothed true model (sigma 15)",
                                                ckpt_every=K, checkpoint_gb=round(prob.checkpoint_bytes() / 1e9, 2),
-                                               launch_shape=tune),
+                                               launch_shape=dict(rtm=tune, gradient=prob.tune)),
                 gcell_upd_per_s=round(2 * cells * nt / (ms / 1000.0) / 1e9, 2), misfit=J,
                 normalized_corr_gradient_vs_reference_rtm_image=corr,
                 note="finite-difference (FP64, 10 directions) and dot-product checks: tests/test_gpu_adjoint.py")
@@ -141,7 +141,7 @@ def run_c5(args):
         resid = (syn - obs)
         rtm.close()
         prob = FWIProblem(sv.nx, sv.nz, sv.dx, sv.dz, sv.fs, nt, sv.fw, shots, wav, ckpt_every=K,
-                          ckpt_dtype="f16", tune=tune, device=dev)
+                          ckpt_dtype="f16", tune="auto", device=dev)
         lam, mu, rho = (torch.as_tensor(x, device=dev) for x in (t_mig[1], t_mig[0], t_mig[2]))
         a.record()
         d, ck, fl = prob.forward(lam, mu, rho)
@@ -149,6 +149,7 @@ def run_c5(args):
         b.record()
         torch.cuda.synchronize()
         t_grad += a.elapsed_time(b)
+        grad_tune = prob.tune
         grad = g if grad is None else grad + g
         del ck
         prob.close()
@@ -182,7 +183,7 @@ def run_c5(args):
                 config=dict(workload=f"c5: {n} shots, 4001x1601, dx=5 m, dt=0.4 ms, nt={nt}, U{{1000..2000}} receivers, "
                                      f"waves of {wave} shots, FP16 per-field-scaled checkpoints every {K} steps, "
                                      f"isnap={isnap}, Kahan images/gradients, FP64 cross-shot sums",
-                            launch_shape=tune),
+                            launch_shape=dict(rtm=tune, gradient=grad_tune)),
                 rtm_shots_per_s=round(n / (t_rtm / 1000), 4), gradient_shots_per_s=round(n / (t_grad / 1000), 4),
                 rtm_gcell_upd_per_s=round(2 * cells * nt / (t_rtm / 1000) / 1e9, 2),
                 peak_device_memory_gb=round(peak_mem / 1e9, 1), errors=errs,

@@ -62,20 +62,21 @@ struct AdjParams {
     int n;                    // forward step reversed by this launch
 };
 
-// Initial adjoint state a_{nt-1} = R^T g_{nt-1}: one thread per shot adds the
-// last residual sample at its receivers, in receiver order (duplicates at one
-// cell accumulate deterministically).  resid_t is time-major, 3 planes of
-// (nt, nrec_total).
+// Initial adjoint state a_{nt-1} = R^T g_{nt-1}: the last residual sample is
+// added at the receivers.  One thread per (row, shot = blockIdx.y) walks its
+// row's receivers in order, so duplicates at one cell accumulate in receiver
+// order (deterministic); different rows are different cells.  resid_t is
+// time-major, 3 planes of (nt, nrec_total).
 static __global__ void inject_last_resid_kernel(const ShotDev *__restrict__ shots, int nshots,
                                                 const int *__restrict__ rec_ptr, const int2 *__restrict__ rec_ent,
                                                 const float *__restrict__ resid_t, int nt, int nrec_total,
                                                 int nz, int pitch, float *au, float *aw) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = blockIdx.y;
     if (s >= nshots) return;
     (void)nz;
     const ShotDev sh = shots[s];
     const size_t plane = (size_t)nt * nrec_total;
-    for (int i = 0; i < sh.nx; ++i)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < sh.nx; i += gridDim.x * blockDim.x)
         for (int e = rec_ptr[sh.rec_row0 + i]; e < rec_ptr[sh.rec_row0 + i + 1]; ++e) {
             const int2 en = rec_ent[e];
             const long long o = sh.state_off + (long long)(i + 1) * pitch + en.x + COL_OFF;

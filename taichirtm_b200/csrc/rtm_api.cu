@@ -978,7 +978,9 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
         auto fld = [&](float *base, int f) { return base + (size_t)f * sf; };
         // a_{nt-1} = R^T g_{nt-1}
         if (p->nrec_total) {
-            inject_last_resid_kernel<<<(p->nshots + 127) / 128, 128, 0, s>>>(
+            int max_nx = 1;
+            for (const ShotDev &d : p->shots_h) max_nx = std::max(max_nx, d.nx);
+            inject_last_resid_kernel<<<dim3((max_nx + 127) / 128, p->nshots), 128, 0, s>>>(
                 p->d_shots, p->nshots, p->d_rec_ptr, p->d_rec_ent, p->d_obs_t, nt, p->nrec_total,
                 p->g.nz, p->pitch, fld(adj[0], A_U), fld(adj[0], A_W));
             CUDA_TRY(cudaGetLastError());

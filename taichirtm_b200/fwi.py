@@ -27,8 +27,20 @@ class FWIProblem:
 
     def __init__(self, nx, nz, dx, dz, fs, nt, absorbing_frame, shots, wavelets, ckpt_every=None,
                  surface=None, tune=None, device=None, ckpt_dtype="f32"):
+        """tune: launch shape dict, None (library default) or "auto" (timed on
+        short gradients of this acquisition, cached per GPU and geometry)."""
         self.device = torch.device(device if device is not None else "cuda")
         self.nx, self.nz, self.nt = int(nx), int(nz), int(nt)
+        if tune == "auto":  # time candidate launch shapes on short gradients (cached)
+            from . import autotune
+
+            def make(t, steps):
+                w = to_tensor(wavelets, torch.float32, self.device)[..., :steps].contiguous()
+                return FWIProblem(nx, nz, dx, dz, fs, steps, absorbing_frame, shots, w,
+                                  ckpt_every=max(1, round(math.sqrt(steps))), surface=surface, tune=t,
+                                  device=self.device, ckpt_dtype=ckpt_dtype)
+            tune = autotune.best_fwi_shape(make, self.nx, self.nz, list(shots)) if self.nt >= autotune.FWI_TUNE_STEPS else None
+        self.tune = tune
         self.plan = Plan(nx, nz, dx, dz, nt, fs, absorbing_frame, PSV, list(shots), tune=tune,
                          device=self.device)
         self.wavelets = to_tensor(wavelets, torch.float32, self.device)
