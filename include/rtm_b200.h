@@ -74,8 +74,10 @@ typedef struct {
     int rows;       /* rows per warp task */
     int warps;      /* warps per CTA */
     int prefetch;   /* 1: software-pipelined row loads; 3: cp.async pipeline, rows 3 ahead in a
-                       per-warp shared-memory ring; 2: row loads plus L2 cache policies (state
-                       evict-first, material evict-last); 0: plain; other values = default (1) */
+                       per-warp shared-memory ring (with tsteps 2: the material and 1/rho rows
+                       through a 4-row ring, the state in registers); 2: row loads plus L2 cache
+                       policies (state evict-first, material evict-last); 0: plain; other values =
+                       default (1) */
     int graphs;     /* 1: capture each time loop as a CUDA graph on first use and replay it
                        while its pointers and schedule stay the same; 0 = direct launches */
     int tsteps;     /* time steps per launch of rtm_forward, rtm_backward and the

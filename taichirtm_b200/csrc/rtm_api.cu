@@ -213,19 +213,41 @@ cudaError_t launch_mode(const StepParams &sp, int modes, int vec, int warps, cud
     }
 }
 
-template <int DIR, int MODE, int VEC>
+template <int DIR, int MODE, int VEC, bool RING>
 cudaError_t launch_step2(const StepParams &sp, int warps, cudaStream_t s) {
-    step2_kernel<DIR, MODE, VEC><<<(sp.n_work + warps - 1) / warps, 32 * warps, 0, s>>>(sp);
+    size_t smem = 0;
+    if constexpr (RING) {
+        constexpr size_t kMaxSmem = 227 * 1024;  // per-block opt-in limit
+        smem = (size_t)warps * ring2_smem_per_warp<MODE, VEC>();
+        if (smem > kMaxSmem) return cudaErrorInvalidConfiguration;
+        static bool attr_set = false;  // per instantiation; raises the 48 KB default
+        if (!attr_set) {
+            const size_t want = std::min<size_t>(8 * ring2_smem_per_warp<MODE, VEC>(), kMaxSmem);
+            cudaError_t e = cudaFuncSetAttribute(step2_kernel<DIR, MODE, VEC, RING>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
+            if (e != cudaSuccess) return e;
+            attr_set = true;
+        }
+    }
+    step2_kernel<DIR, MODE, VEC, RING><<<(sp.n_work + warps - 1) / warps, 32 * warps, smem, s>>>(sp);
     return cudaGetLastError();
 }
 
-// Two steps (sp.it, sp.it2) in one launch; vec is 2 or 4 (checked at plan creation).
+template <int DIR, int MODE>
+cudaError_t launch_vec2(const StepParams &sp, int vec, bool ring, int warps, cudaStream_t s) {
+    if (vec == 2) return ring ? launch_step2<DIR, MODE, 2, true>(sp, warps, s) : launch_step2<DIR, MODE, 2, false>(sp, warps, s);
+    return ring ? launch_step2<DIR, MODE, 4, true>(sp, warps, s) : launch_step2<DIR, MODE, 4, false>(sp, warps, s);
+}
+
+// Two steps (sp.it, sp.it2) in one launch; vec is 2 or 4 (checked at plan
+// creation); prefetch 3 selects the shared-memory material ring.
 template <int DIR>
-cudaError_t launch_mode2(const StepParams &sp, int modes, int vec, int warps, cudaStream_t s) {
+cudaError_t launch_mode2(const StepParams &sp, int modes, int vec, int prefetch, int warps, cudaStream_t s) {
+    const bool ring = prefetch == 3;
     switch (modes) {
-        case RTM_PSV: return vec == 2 ? launch_step2<DIR, RTM_PSV, 2>(sp, warps, s) : launch_step2<DIR, RTM_PSV, 4>(sp, warps, s);
-        case RTM_SH: return vec == 2 ? launch_step2<DIR, RTM_SH, 2>(sp, warps, s) : launch_step2<DIR, RTM_SH, 4>(sp, warps, s);
-        default: return vec == 2 ? launch_step2<DIR, RTM_BOTH, 2>(sp, warps, s) : launch_step2<DIR, RTM_BOTH, 4>(sp, warps, s);
+        case RTM_PSV: return launch_vec2<DIR, RTM_PSV>(sp, vec, ring, warps, s);
+        case RTM_SH: return launch_vec2<DIR, RTM_SH>(sp, vec, ring, warps, s);
+        default: return launch_vec2<DIR, RTM_BOTH>(sp, vec, ring, warps, s);
     }
 }
 
@@ -581,7 +603,7 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
                 sp.it2 = it + 1;
                 sp.snap_k2 = snap_at(it + 1);
                 sp.check = check_at(it + 1);
-                CUDA_TRY((launch_mode2<0>(sp, p->g.modes, p->vec, p->warps, ls)));
+                CUDA_TRY((launch_mode2<0>(sp, p->g.modes, p->vec, p->prefetch, p->warps, ls)));
             } else {
                 sp.check = check_at(it);
                 CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, ls)));
@@ -676,7 +698,7 @@ static int backward_impl(rtm_plan *p, const float *obs, const float *snap_u, con
                 sp.it2 = (nt - 1) - (it + 1);
                 sp.snap_k2 = snap_of[it + 1];
                 sp.check = check_at(it + 1);
-                CUDA_TRY((launch_mode2<1>(sp, p->g.modes, p->vec, p->warps, ls)));
+                CUDA_TRY((launch_mode2<1>(sp, p->g.modes, p->vec, p->prefetch, p->warps, ls)));
             } else {
                 sp.check = check_at(it);
                 CUDA_TRY((launch_mode<1>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, ls)));
@@ -906,7 +928,7 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
         if (ln.two) {
             sp.it2 = last;
             sp.snap_k2 = -1;
-            CUDA_TRY((launch_mode2<0>(sp, p->g.modes, p->vec, p->warps, s)));
+            CUDA_TRY((launch_mode2<0>(sp, p->g.modes, p->vec, p->prefetch, p->warps, s)));
         } else {
             CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, s)));
         }
@@ -1180,7 +1202,7 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
                 if (fsched[L].two) {
                     fp.it2 = it + 1;
                     fp.snap_k2 = slot_at(it + 1);
-                    CUDA_TRY((launch_mode2<0>(fp, RTM_PSV, p->vec, p->warps, s)));
+                    CUDA_TRY((launch_mode2<0>(fp, RTM_PSV, p->vec, p->prefetch, p->warps, s)));
                 } else {
                     CUDA_TRY((launch_mode<0>(fp, RTM_PSV, p->vec | (p->prefetch << 8), p->warps, s)));
                 }
@@ -1202,7 +1224,7 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
                     bp.it2 = t - 1;
                     bp.snap_k2 = slot_at(t - 1);
                     bp.check = check_at(it + 1);
-                    CUDA_TRY((launch_mode2<1>(bp, RTM_PSV, p->vec, p->warps, s)));
+                    CUDA_TRY((launch_mode2<1>(bp, RTM_PSV, p->vec, p->prefetch, p->warps, s)));
                 } else {
                     bp.check = check_at(it);
                     CUDA_TRY((launch_mode<1>(bp, RTM_PSV, p->vec | (p->prefetch << 8), p->warps, s)));

@@ -72,7 +72,22 @@ __device__ __forceinline__ void ldv_coherent(float (&v)[VEC], float *p) {
     }
 }
 
-template <int DIR, int MODE, int VEC>
+// Material ring (RING = true): the material and inverse-density rows reach a
+// warp through a per-warp shared-memory ring of RING2_ROWS rows, filled by
+// cp.async one iteration ahead, instead of rolling through registers.  Each
+// lane copies and reads back only its own VEC columns, so its own
+// wait_group is the only synchronisation.  It frees about 30 registers per
+// thread, i.e. more resident warps.  Fields per ring row: P-SV lam, mu, mxz,
+// 1/rho_u, 1/rho_w; SH myx, myz, 1/rho; the surface mask.
+constexpr int RING2_ROWS = 4;
+template <int MODE>
+__host__ __device__ constexpr int ring2_fields() { return ((MODE & 1) ? 5 : 0) + ((MODE & 2) ? 3 : 0) + 1; }
+template <int MODE, int VEC>
+__host__ __device__ constexpr size_t ring2_smem_per_warp() {
+    return (size_t)RING2_ROWS * ring2_fields<MODE>() * 32 * VEC * sizeof(float);
+}
+
+template <int DIR, int MODE, int VEC, bool RING = false>
 __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     static_assert(VEC >= 2, "two steps per launch need two halo columns per side");
     constexpr bool PSV = (MODE & 1) != 0;
@@ -132,6 +147,56 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
             for (int q = 0; q < VEC; ++q) m.sm[q] = 1.f;
         }
     };
+    // ---- material ring (RING): slot of a row, copy-in, read-back
+    constexpr int NRF = ring2_fields<MODE>();
+    constexpr int RF_LAM = 0, RF_MU = 1, RF_MXZ = 2, RF_IRU = 3, RF_IRW = 4;
+    constexpr int RF_MYX = PSV ? 5 : 0, RF_MYZ = RF_MYX + 1, RF_IR = RF_MYX + 2;
+    constexpr int RF_SM = NRF - 1;
+    extern __shared__ float step2_smem[];
+    float *ring = step2_smem + (size_t)(threadIdx.x >> 5) * (RING2_ROWS * NRF * 32 * VEC);
+    auto rslot = [&](int row, int f) {
+        const int s = (row + 4 * RING2_ROWS) % RING2_ROWS;  // rows >= -2
+        return ring + ((size_t)(s * NRF + f) * 32 + lane) * VEC;
+    };
+    auto ring_issue = [&](int row) {
+        auto put = [&](int f, const float *src) {
+            if (row_ok(row)) {
+                cp_async_vec<VEC>(rslot(row, f), src + moff + (long long)(row + 1) * P);
+            } else {
+                float *d = rslot(row, f);
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) d[q] = 0.f;  // rows beyond the pads read as zero
+            }
+        };
+        if constexpr (PSV) {
+            put(RF_LAM, p.mat[M_LAM]); put(RF_MU, p.mat[M_MU]); put(RF_MXZ, p.mat[M_MXZ]);
+            put(RF_IRU, p.mat[M_IRU]); put(RF_IRW, p.mat[M_IRW]);
+        }
+        if constexpr (SH) { put(RF_MYX, p.mat[M_MYX]); put(RF_MYZ, p.mat[M_MYZ]); put(RF_IR, p.mat[M_IR]); }
+        if (p.surface) put(RF_SM, p.surface);
+        cp_async_commit();  // one group per issued row, so the group counts stay aligned
+    };
+    auto rd_ring = [&](int row, int f, float (&v)[VEC]) {
+        const float *s = rslot(row, f);
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) v[q] = s[q];
+    };
+    auto ring_ir = [&](int row, Vel &v) {
+        if constexpr (PSV) { rd_ring(row, RF_IRU, v.u); rd_ring(row, RF_IRW, v.w); }
+        if constexpr (SH) rd_ring(row, RF_IR, v.v);
+    };
+    auto ring_mat = [&](int row, Mat &m) {
+        if constexpr (PSV) { rd_ring(row, RF_LAM, m.lam); rd_ring(row, RF_MU, m.mu); rd_ring(row, RF_MXZ, m.mxz); }
+        if constexpr (SH) { rd_ring(row, RF_MYX, m.myx); rd_ring(row, RF_MYZ, m.myz); }
+        if (p.surface) {
+            rd_ring(row, RF_SM, m.sm);
+        } else {
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) m.sm[q] = 1.f;
+        }
+    };
+    (void)ring_issue; (void)ring_ir; (void)ring_mat;
+
     auto cp_sig = [&](Sig &d, const Sig &s) {
         if constexpr (PSV) { copy_arr<VEC>(d.xx, s.xx); copy_arr<VEC>(d.zz, s.zz); copy_arr<VEC>(d.xz, s.xz); }
         if constexpr (SH) { copy_arr<VEC>(d.yx, s.yx); copy_arr<VEC>(d.yz, s.yz); }
@@ -444,86 +509,185 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     };
 
     const int tA = p.it, tB = p.it2;
-    // rolling rows (see the header comment for which row each holds)
-    Sig so_p, so_c, sa_p, sa_c, s_out, n_so;
-    Vel va_p, va_c, vb_p, vb_c, vo, ir_p, ir_c, vabs_c, v_out, n_vo, n_ir;
-    Mat m_p, m_c, n_m;
-    zero_sig(sa_p); zero_sig(sa_c);
-    zero_vel(va_p); zero_vel(vb_p); zero_vel(vabs_c);
-    load_sig(ia - 2, so_p);
-
-    if constexpr (DIR == 0) {
-        // iteration k: A velocity k, A stress k-1, B velocity k-1, B stress k-2
-        // prefetched per iteration: old stress, old velocity, 1/rho of row k+1; material of row k
-        load_sig(ia - 1, n_so);
-        load_vel(ia - 1, n_vo);
-        load_ir(ia - 1, n_ir);
-        load_mat(ia - 2, n_m);
-        for (int k = ia - 1; k <= ib + 1; ++k) {
-            cp_sig(so_c, n_so);
-            cp_vel(vo, n_vo);
-            cp_vel(ir_c, n_ir);
-            cp_mat(m_c, n_m);  // row k-1
-            if (k <= ib) {
-                load_sig(k + 1, n_so);
-                load_vel(k + 1, n_vo);
-                load_ir(k + 1, n_ir);
-                load_mat(k, n_m);
+    if constexpr (RING) {
+        // rolling rows as in the register version below, minus 1/rho and the
+        // material, which come from the ring at the point of use
+        Sig so_p, so_c, sa_p, sa_c, s_out, n_so;
+        Vel va_p, va_c, vb_p, vb_c, vo, vabs_c, vabs_p, v_out, n_vo;
+        zero_sig(sa_p); zero_sig(sa_c);
+        zero_vel(va_p); zero_vel(vb_p); zero_vel(vabs_c); zero_vel(vabs_p);
+        load_sig(ia - 2, so_p);
+        if constexpr (DIR == 0) {
+            // iteration k: A velocity k, A stress k-1, B velocity k-1, B stress k-2;
+            // ring rows read: k (1/rho), k-1 (1/rho, material), k-2 (material);
+            // issued: row k+1 into the slot of row k-3
+            load_sig(ia - 1, n_so);
+            load_vel(ia - 1, n_vo);
+            ring_issue(ia - 2);
+            ring_issue(ia - 1);
+            for (int k = ia - 1; k <= ib + 1; ++k) {
+                cp_sig(so_c, n_so);
+                cp_vel(vo, n_vo);
+                if (k <= ib) {
+                    load_sig(k + 1, n_so);
+                    load_vel(k + 1, n_vo);
+                }
+                ring_issue(k + 1);
+                cp_async_wait<1>();  // every row up to k has landed
+                {
+                    Vel ir;
+                    ring_ir(k, ir);
+                    vel_update(k, tA, so_c, so_p, vo, ir, va_c);
+                }
+                if (k >= ia) {
+                    Mat m;
+                    ring_mat(k - 1, m);
+                    stress_update(k - 1, va_p, va_c, so_p, m, sa_c, vabs_c);
+                    if (owner && k - 1 >= ia && k - 1 < ib) epilogue(k - 1, tA, p.snap_k, vabs_c);
+                }
+                if (k >= ia + 1) {
+                    Vel ir;
+                    ring_ir(k - 1, ir);
+                    vel_update(k - 1, tB, sa_c, sa_p, vabs_c, ir, vb_c);
+                }
+                if (k >= ia + 2) {
+                    Mat m;
+                    ring_mat(k - 2, m);
+                    stress_update(k - 2, vb_p, vb_c, sa_p, m, s_out, v_out);
+                    finish_b(k - 2, s_out, v_out);
+                }
+                cp_sig(so_p, so_c);
+                cp_vel(va_p, va_c);
+                cp_sig(sa_p, sa_c);
+                cp_vel(vb_p, vb_c);
             }
-            vel_update(k, tA, so_c, so_p, vo, ir_c, va_c);
-            if (k >= ia) {
-                stress_update(k - 1, va_p, va_c, so_p, m_c, sa_c, vabs_c);
-                if (owner && k - 1 >= ia && k - 1 < ib) epilogue(k - 1, tA, p.snap_k, vabs_c);
+        } else {
+            // iteration k: A velocity k-1, A stress k-1, B velocity k-2, B stress k-2;
+            // ring rows read: k-1, k-2; issued: row k into the slot of row k-4
+            load_sig(ia - 1, n_so);
+            load_vel(ia - 2, n_vo);
+            ring_issue(ia - 2);
+            for (int k = ia - 1; k <= ib + 1; ++k) {
+                cp_sig(so_c, n_so);   // row k
+                cp_vel(vo, n_vo);     // row k-1
+                if (k <= ib) {
+                    load_sig(k + 1, n_so);
+                    load_vel(k, n_vo);
+                }
+                ring_issue(k);
+                cp_async_wait<1>();  // every row up to k-1 has landed
+                {
+                    Vel ir;
+                    ring_ir(k - 1, ir);
+                    vel_update(k - 1, tA, so_c, so_p, vo, ir, va_c);
+                }
+                if (k >= ia) {
+                    Mat m;
+                    ring_mat(k - 1, m);
+                    stress_update(k - 1, va_c, va_p, so_p, m, sa_c, vabs_c);
+                    if (owner && k - 1 >= ia && k - 1 < ib) epilogue(k - 1, tA, p.snap_k, vabs_c);
+                }
+                if (k >= ia + 1) {
+                    Vel ir;
+                    ring_ir(k - 2, ir);
+                    vel_update(k - 2, tB, sa_c, sa_p, vabs_p, ir, vb_c);
+                }
+                if (k >= ia + 2) {
+                    Mat m;
+                    ring_mat(k - 2, m);
+                    stress_update(k - 2, vb_c, vb_p, sa_p, m, s_out, v_out);
+                    finish_b(k - 2, s_out, v_out);
+                }
+                cp_sig(so_p, so_c);
+                cp_vel(va_p, va_c);
+                cp_sig(sa_p, sa_c);
+                cp_vel(vabs_p, vabs_c);
+                cp_vel(vb_p, vb_c);
             }
-            if (k >= ia + 1) vel_update(k - 1, tB, sa_c, sa_p, vabs_c, ir_p, vb_c);
-            if (k >= ia + 2) {
-                stress_update(k - 2, vb_p, vb_c, sa_p, m_p, s_out, v_out);
-                finish_b(k - 2, s_out, v_out);
-            }
-            cp_sig(so_p, so_c);
-            cp_vel(va_p, va_c);
-            cp_sig(sa_p, sa_c);
-            cp_vel(vb_p, vb_c);
-            cp_vel(ir_p, ir_c);
-            cp_mat(m_p, m_c);
         }
+        cp_async_wait<0>();  // no copy outlives the kernel
     } else {
-        // iteration k: A velocity k-1, A stress k-1, B velocity k-2, B stress k-2
-        // prefetched per iteration: old stress of row k+1; old velocity, 1/rho, material of row k
-        Vel vabs_p;
-        zero_vel(vabs_p);
-        load_sig(ia - 1, n_so);
-        load_vel(ia - 2, n_vo);
-        load_ir(ia - 2, n_ir);
-        load_mat(ia - 2, n_m);
-        for (int k = ia - 1; k <= ib + 1; ++k) {
-            cp_sig(so_c, n_so);   // row k
-            cp_vel(vo, n_vo);     // row k-1
-            cp_vel(ir_c, n_ir);   // row k-1
-            cp_mat(m_c, n_m);     // row k-1
-            if (k <= ib) {
-                load_sig(k + 1, n_so);
-                load_vel(k, n_vo);
-                load_ir(k, n_ir);
-                load_mat(k, n_m);
+        // rolling rows (see the header comment for which row each holds)
+        Sig so_p, so_c, sa_p, sa_c, s_out, n_so;
+        Vel va_p, va_c, vb_p, vb_c, vo, ir_p, ir_c, vabs_c, v_out, n_vo, n_ir;
+        Mat m_p, m_c, n_m;
+        zero_sig(sa_p); zero_sig(sa_c);
+        zero_vel(va_p); zero_vel(vb_p); zero_vel(vabs_c);
+        load_sig(ia - 2, so_p);
+
+        if constexpr (DIR == 0) {
+            // iteration k: A velocity k, A stress k-1, B velocity k-1, B stress k-2
+            // prefetched per iteration: old stress, old velocity, 1/rho of row k+1; material of row k
+            load_sig(ia - 1, n_so);
+            load_vel(ia - 1, n_vo);
+            load_ir(ia - 1, n_ir);
+            load_mat(ia - 2, n_m);
+            for (int k = ia - 1; k <= ib + 1; ++k) {
+                cp_sig(so_c, n_so);
+                cp_vel(vo, n_vo);
+                cp_vel(ir_c, n_ir);
+                cp_mat(m_c, n_m);  // row k-1
+                if (k <= ib) {
+                    load_sig(k + 1, n_so);
+                    load_vel(k + 1, n_vo);
+                    load_ir(k + 1, n_ir);
+                    load_mat(k, n_m);
+                }
+                vel_update(k, tA, so_c, so_p, vo, ir_c, va_c);
+                if (k >= ia) {
+                    stress_update(k - 1, va_p, va_c, so_p, m_c, sa_c, vabs_c);
+                    if (owner && k - 1 >= ia && k - 1 < ib) epilogue(k - 1, tA, p.snap_k, vabs_c);
+                }
+                if (k >= ia + 1) vel_update(k - 1, tB, sa_c, sa_p, vabs_c, ir_p, vb_c);
+                if (k >= ia + 2) {
+                    stress_update(k - 2, vb_p, vb_c, sa_p, m_p, s_out, v_out);
+                    finish_b(k - 2, s_out, v_out);
+                }
+                cp_sig(so_p, so_c);
+                cp_vel(va_p, va_c);
+                cp_sig(sa_p, sa_c);
+                cp_vel(vb_p, vb_c);
+                cp_vel(ir_p, ir_c);
+                cp_mat(m_p, m_c);
             }
-            vel_update(k - 1, tA, so_c, so_p, vo, ir_c, va_c);
-            if (k >= ia) {
-                stress_update(k - 1, va_c, va_p, so_p, m_c, sa_c, vabs_c);
-                if (owner && k - 1 >= ia && k - 1 < ib) epilogue(k - 1, tA, p.snap_k, vabs_c);
+        } else {
+            // iteration k: A velocity k-1, A stress k-1, B velocity k-2, B stress k-2
+            // prefetched per iteration: old stress of row k+1; old velocity, 1/rho, material of row k
+            Vel vabs_p;
+            zero_vel(vabs_p);
+            load_sig(ia - 1, n_so);
+            load_vel(ia - 2, n_vo);
+            load_ir(ia - 2, n_ir);
+            load_mat(ia - 2, n_m);
+            for (int k = ia - 1; k <= ib + 1; ++k) {
+                cp_sig(so_c, n_so);   // row k
+                cp_vel(vo, n_vo);     // row k-1
+                cp_vel(ir_c, n_ir);   // row k-1
+                cp_mat(m_c, n_m);     // row k-1
+                if (k <= ib) {
+                    load_sig(k + 1, n_so);
+                    load_vel(k, n_vo);
+                    load_ir(k, n_ir);
+                    load_mat(k, n_m);
+                }
+                vel_update(k - 1, tA, so_c, so_p, vo, ir_c, va_c);
+                if (k >= ia) {
+                    stress_update(k - 1, va_c, va_p, so_p, m_c, sa_c, vabs_c);
+                    if (owner && k - 1 >= ia && k - 1 < ib) epilogue(k - 1, tA, p.snap_k, vabs_c);
+                }
+                if (k >= ia + 1) vel_update(k - 2, tB, sa_c, sa_p, vabs_p, ir_p, vb_c);
+                if (k >= ia + 2) {
+                    stress_update(k - 2, vb_c, vb_p, sa_p, m_p, s_out, v_out);
+                    finish_b(k - 2, s_out, v_out);
+                }
+                cp_sig(so_p, so_c);
+                cp_vel(va_p, va_c);
+                cp_sig(sa_p, sa_c);
+                cp_vel(vabs_p, vabs_c);
+                cp_vel(vb_p, vb_c);
+                cp_vel(ir_p, ir_c);
+                cp_mat(m_p, m_c);
             }
-            if (k >= ia + 1) vel_update(k - 2, tB, sa_c, sa_p, vabs_p, ir_p, vb_c);
-            if (k >= ia + 2) {
-                stress_update(k - 2, vb_c, vb_p, sa_p, m_p, s_out, v_out);
-                finish_b(k - 2, s_out, v_out);
-            }
-            cp_sig(so_p, so_c);
-            cp_vel(va_p, va_c);
-            cp_sig(sa_p, sa_c);
-            cp_vel(vabs_p, vabs_c);
-            cp_vel(vb_p, vb_c);
-            cp_vel(ir_p, ir_c);
-            cp_mat(m_p, m_c);
         }
     }
     if (p.check) {

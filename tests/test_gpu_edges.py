@@ -75,7 +75,7 @@ def test_shot_without_sources_or_receivers(case, tune):
 
 
 @pytest.mark.parametrize("tune", [dict(vec=1, rows=1, warps=1, prefetch=0), dict(vec=2, rows=2, warps=1, tsteps=2),
-                                  dict(vec=4, rows=8, warps=4, prefetch=3)])
+                                  dict(vec=4, rows=8, warps=4, prefetch=3), dict(vec=2, rows=2, warps=3, tsteps=2, prefetch=3)])
 @pytest.mark.parametrize("grid", [(3, 3, 0), (5, 4, 0), (23, 17, 0), (23, 17, 4)])
 def test_smallest_grids_and_no_sponge(grid, tune):
     nx, nz, fw = grid
@@ -93,8 +93,8 @@ def test_smallest_grids_and_no_sponge(grid, tune):
     assert np.abs(g["seis"]).max() > 0
 
 
-@pytest.mark.parametrize("tsteps", [1, 2])
-def test_windows_touching_the_model_edges(tsteps):
+@pytest.mark.parametrize("tsteps,prefetch", [(1, 1), (2, 1), (2, 3)])
+def test_windows_touching_the_model_edges(tsteps, prefetch):
     """Windows [0, 40), [60, 100) (the last rows) and [0, 100) in one batched
     plan equal standalone runs on the cropped models, bit for bit."""
     from taichirtm_b200.plan import Plan, ShotGeometry
@@ -109,7 +109,7 @@ def test_windows_touching_the_model_edges(tsteps):
         wv = np.zeros((3, 3, nt), np.float32)
         wv[:, :] = _ricker(nt)[None, None]
         wav.append(wv)
-    tune = dict(vec=2, rows=3, warps=2, tsteps=tsteps)
+    tune = dict(vec=2, rows=3, warps=2, tsteps=tsteps, prefetch=prefetch)
     p = Plan(nx, nz, 4.0, 4.0, nt, 2000.0, fw, 1, shots, tune=tune)
     p.set_model(mu, lam, rho)
     f, seis, _, _ = p.forward(torch.as_tensor(np.concatenate(wav, axis=1)))

@@ -87,7 +87,9 @@ def _same(a, b):
 
 @pytest.mark.parametrize("modes", [1, 2, 3])
 @pytest.mark.parametrize("tune", [dict(vec=2, rows=7, warps=3), dict(vec=4, rows=16, warps=2),
-                                  dict(vec=2, rows=1, warps=4), dict(vec=4, rows=2, warps=1)])
+                                  dict(vec=2, rows=1, warps=4), dict(vec=4, rows=2, warps=1),
+                                  dict(vec=2, rows=5, warps=2, prefetch=3), dict(vec=4, rows=3, warps=1, prefetch=3),
+                                  dict(vec=2, rows=1, warps=8, prefetch=3)])
 def test_two_steps_per_launch_bit_identical(modes, tune):
     C = _case()
     one = _run(C, modes, dict(tune, tsteps=1), isnap=3)
@@ -97,14 +99,15 @@ def test_two_steps_per_launch_bit_identical(modes, tune):
     assert two["launches"] < one["launches"]
 
 
+@pytest.mark.parametrize("prefetch", [1, 3])
 @pytest.mark.parametrize("isnap", [1, 2])
-def test_two_steps_imaging_every_step_and_topography(isnap):
+def test_two_steps_imaging_every_step_and_topography(isnap, prefetch):
     C = _case(nx=90, nz=130, nt=40, fw=12, seed=5)
     sm = _topography(C["nx"], C["nz"])
     one = _run(C, 1, dict(vec=2, rows=5, warps=2, tsteps=1), isnap=isnap, check=1, surface=sm)
-    two = _run(C, 1, dict(vec=2, rows=5, warps=2, tsteps=2), isnap=isnap, check=1, surface=sm)
+    two = _run(C, 1, dict(vec=2, rows=5, warps=2, tsteps=2, prefetch=prefetch), isnap=isnap, check=1, surface=sm)
     _same(one, two)
-    two = _run(C, 1, dict(vec=2, rows=5, warps=2, tsteps=2), isnap=isnap, check=0, surface=sm)
+    two = _run(C, 1, dict(vec=2, rows=5, warps=2, tsteps=2, prefetch=prefetch), isnap=isnap, check=0, surface=sm)
     _same(one, two)
 
 
@@ -137,7 +140,8 @@ def _batched(tsteps, checkpoint=None, modes=1):
     wv[2] = np.stack(wav)
     wv[0] = 0.3 * wv[2]
     b = BatchedRTM(mu, lam, rho, 4.0, 4.0, 2000.0, nt, fw, shots, modes=modes,
-                   tune=dict(vec=2, rows=9, warps=2, tsteps=tsteps), graphs=tsteps == 2)
+                   tune=dict(vec=2, rows=9, warps=2, tsteps=tsteps, prefetch=3 if tsteps == 2 else 1),
+                   graphs=tsteps == 2)
     ff, seis, _, _ = b.forward(wv, check_interval=10)
     obs = seis * 0.7
     out = b.migrate(wv, obs, isnap=3, check_interval=10, checkpoint=checkpoint)
@@ -199,7 +203,7 @@ def test_failing_check_step_is_complete_for_every_launch_shape():
     outs = []
     for tune in (dict(vec=2, rows=4, warps=2, tsteps=1), dict(vec=2, rows=4, warps=2, tsteps=2),
                  dict(vec=1, rows=3, warps=1, prefetch=0), dict(vec=4, rows=64, warps=8, prefetch=3),
-                 dict(vec=4, rows=2, warps=8, tsteps=2)):
+                 dict(vec=4, rows=2, warps=8, tsteps=2), dict(vec=2, rows=6, warps=2, tsteps=2, prefetch=3)):
         p = Plan(C["nx"], C["nz"], C["dx"], C["dz"], C["nt"], C["fs"], C["fw"], 1,
                  [ShotGeometry(0, C["nx"], src, C["rec"])], tune=tune)
         p.set_model(mu, lam, rho)
