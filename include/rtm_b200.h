@@ -237,6 +237,19 @@ long long rtm_plan_launch_count(const rtm_plan *plan);
 const char *rtm_last_error(void);
 const char *rtm_version(void);
 
+/* Bounds-checking build (librtm_b200_debug.so, compiled with
+ * -DRTM_BOUNDS_CHECK).  In that build every global access of the propagation
+ * and adjoint kernels is checked against the device buffers of the current
+ * call.  An access outside all of them is skipped and counted, and the entry
+ * point returns RTM_E_CUDA.
+ * rtm_bounds_probe says whether [ptr, ptr + bytes) lies inside one of the
+ * plan's buffers or the caller buffer [buf, buf + buf_bytes), as the kernels'
+ * checks see it (nothing is read at ptr); *inside (host) receives 1 or 0.
+ * The normal build returns RTM_E_STATE.  No reference counterpart (a test
+ * aid standing in for a memory checker). */
+int rtm_bounds_probe(const rtm_plan *plan, const void *buf, size_t buf_bytes, const void *ptr, size_t bytes,
+                     int32_t *inside);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,7 +54,7 @@ def lib():
         return _lib
     override = os.environ.get("TAICHIRTM_B200_LIB")  # a separately built librtm_b200.so
     path = override or _build.LIB
-    if not override and (not os.path.exists(path) or _build._stale()):
+    if not override and (not os.path.exists(path) or _build._stale(path)):
         try:
             path = _build.build()
         except Exception as e:  # no nvcc: fail loudly, there is no CPU path
@@ -73,6 +73,7 @@ def lib():
     _sig(L, "rtm_plan_set_model", c_int, vp, vp, vp, vp, vp, vp)
     _sig(L, "rtm_forward", c_int, vp, vp, vp, c_int, c_int, vp, vp, vp, I32P, c_int, I32P, vp)
     _sig(L, "rtm_backward", c_int, vp, vp, vp, vp, vp, I32P, c_int, c_int, vp, vp, c_int, I32P, vp)
+    _sig(L, "rtm_bounds_probe", c_int, vp, vp, c_size, vp, c_size, I32P)
     _sig(L, "rtm_backward_normalized", c_int, vp, vp, vp, vp, vp, I32P, c_int, c_int, ctypes.c_float, vp, vp,
          c_int, I32P, vp)
     _sig(L, "rtm_plan_state_floats", c_size, vp)

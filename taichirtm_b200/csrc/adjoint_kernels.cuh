@@ -81,6 +81,9 @@ static __global__ void inject_last_resid_kernel(const ShotDev *__restrict__ shot
             const int2 en = rec_ent[e];
             const long long o = sh.state_off + (long long)(i + 1) * pitch + en.x + COL_OFF;
             const size_t t = (size_t)(nt - 1) * nrec_total + en.y;
+            if (!RTM_DBG_OK(au + o, 4) || !RTM_DBG_OK(aw + o, 4) || !RTM_DBG_OK(resid_t + t, 4) ||
+                !RTM_DBG_OK(resid_t + 2 * plane + t, 4))
+                continue;
             au[o] += resid_t[t];
             aw[o] += resid_t[2 * plane + t];
         }
@@ -120,7 +123,7 @@ __device__ __forceinline__ float adj_sponge(const float *prof, int fw, int nz, i
     if (i >= 0 && i < fw && db > i) d = i;
     if (dr >= 0 && dr < fw && db > dr) d = dr;
     if (db >= 0 && db < fw && i >= db && dr >= db) d = db;
-    return d >= 0 ? __ldg(prof + d) : 1.0f;
+    return d >= 0 ? ldg_chk(prof + d) : 1.0f;
 }
 
 template <int VEC>
@@ -272,9 +275,9 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
             }
             // sources of row k: recompute injection (fm:421-443)
             if (k < nx && n < p.nt) {
-                const int e0 = __ldg(p.src_ptr + sh.src_row0 + k), e1 = __ldg(p.src_ptr + sh.src_row0 + k + 1);
+                const int e0 = ldg_chk(p.src_ptr + sh.src_row0 + k), e1 = ldg_chk(p.src_ptr + sh.src_row0 + k + 1);
                 for (int e = e0; e < e1; ++e) {
-                    const int2 en = __ldg(p.src_ent + e);
+                    const int2 en = ldg_chk(p.src_ent + e);
                     const int q = en.x - c0;
                     if (q < 0 || q >= VEC) continue;
                     const bool in = interior(k, en.x, nx, nz);
@@ -282,8 +285,8 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
 #pragma unroll
                     for (int qq = 0; qq < VEC; ++qq) {
                         if (qq != q) continue;
-                        up[qq] += __ldg(p.wav[0] + t) * p.src_factor * (in ? bu[qq] : __int_as_float(0x7f800000));
-                        wp[qq] += __ldg(p.wav[2] + t) * p.src_factor * (in ? bw[qq] : __int_as_float(0x7f800000));
+                        up[qq] += ldg_chk(p.wav[0] + t) * p.src_factor * (in ? bu[qq] : __int_as_float(0x7f800000));
+                        wp[qq] += ldg_chk(p.wav[2] + t) * p.src_factor * (in ? bw[qq] : __int_as_float(0x7f800000));
                     }
                 }
             }
@@ -324,10 +327,10 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
             }
             if (owner) {
                 // sources of row r: gradient of the injection scale and wavelet gradient
-                const int e0 = n < p.nt ? __ldg(p.src_ptr + sh.src_row0 + r) : 0;
-                const int e1 = n < p.nt ? __ldg(p.src_ptr + sh.src_row0 + r + 1) : 0;
+                const int e0 = n < p.nt ? ldg_chk(p.src_ptr + sh.src_row0 + r) : 0;
+                const int e1 = n < p.nt ? ldg_chk(p.src_ptr + sh.src_row0 + r + 1) : 0;
                 for (int e = e0; e < e1; ++e) {
-                    const int2 en = __ldg(p.src_ent + e);
+                    const int2 en = ldg_chk(p.src_ent + e);
                     const int q = en.x - c0;
                     if (q < 0 || q >= VEC) continue;
                     const bool in = interior(r, en.x, nx, nz);
@@ -336,29 +339,31 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
 #pragma unroll
                     for (int qq = 0; qq < VEC; ++qq) {
                         if (qq != q || !in) continue;
-                        dbu[qq] += au_p[qq] * (__ldg(p.wav[0] + t) * f);
-                        dbw[qq] += aw_p[qq] * (__ldg(p.wav[2] + t) * f);
+                        dbu[qq] += au_p[qq] * (ldg_chk(p.wav[0] + t) * f);
+                        dbw[qq] += aw_p[qq] * (ldg_chk(p.wav[2] + t) * f);
                         if (p.gwav[0]) {
-                            const float bu_r = __ldg(M(M_IRU, r) + qq), bw_r = __ldg(M(M_IRW, r) + qq);
+                            const float bu_r = ldg_chk(M(M_IRU, r) + qq), bw_r = ldg_chk(M(M_IRW, r) + qq);
                             const size_t g = (size_t)n * p.nsrc_total + en.y;
-                            p.gwav[0][g] += au_p[qq] * f * bu_r;
-                            p.gwav[2][g] += aw_p[qq] * f * bw_r;
+                            if (RTM_DBG_OK(p.gwav[0] + g, 4) && RTM_DBG_OK(p.gwav[2] + g, 4)) {
+                                p.gwav[0][g] += au_p[qq] * f * bu_r;
+                                p.gwav[2][g] += aw_p[qq] * f * bw_r;
+                            }
                         }
                     }
                 }
                 // R^T g_{n-1}: adjoint source at the receivers (fm:445-453 transposed)
                 if (n >= 1) {
-                    const int e0r = __ldg(p.rec_ptr + sh.rec_row0 + r), e1r = __ldg(p.rec_ptr + sh.rec_row0 + r + 1);
+                    const int e0r = ldg_chk(p.rec_ptr + sh.rec_row0 + r), e1r = ldg_chk(p.rec_ptr + sh.rec_row0 + r + 1);
                     for (int e = e0r; e < e1r; ++e) {
-                        const int2 en = __ldg(p.rec_ent + e);
+                        const int2 en = ldg_chk(p.rec_ent + e);
                         const int q = en.x - c0;
                         if (q < 0 || q >= VEC) continue;
                         const size_t t = (size_t)(n - 1) * p.nrec_total + en.y;
 #pragma unroll
                         for (int qq = 0; qq < VEC; ++qq) {
                             if (qq != q) continue;
-                            ou[qq] += __ldg(p.resid[0] + t);
-                            ow[qq] += __ldg(p.resid[2] + t);
+                            ou[qq] += ldg_chk(p.resid[0] + t);
+                            ow[qq] += ldg_chk(p.resid[2] + t);
                         }
                     }
                 }

@@ -1,6 +1,7 @@
 // Host side of librtm_b200: plans, time loops and the extern "C" entry
 // points declared in include/rtm_b200.h.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdarg>
@@ -54,6 +55,13 @@ int dalloc(T **p, size_t n) {
 
 int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
+// NVTX range around an entry point: the phases show up by name in Nsight
+// Systems; without a profiler attached it costs a call that returns.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+
 }  // namespace
 
 struct rtm_plan {
@@ -70,6 +78,7 @@ struct rtm_plan {
     int *d_src_ptr = nullptr, *d_rec_ptr = nullptr;
     int2 *d_src_ent = nullptr, *d_rec_ent = nullptr;
     int nsrc_total = 0, nrec_total = 0;
+    size_t n_src_ptr = 0, n_rec_ptr = 0, n_src_ent = 0, n_rec_ent = 0;  // table lengths
     long long rows_total = 0;  // sum of nx over shots
     size_t state_floats = 0;   // per field, per buffer
     float *d_state[2][NFIELD] = {};
@@ -117,6 +126,70 @@ void plan_free(rtm_plan *p) {
     if (p->ev_out) cudaEventDestroy(p->ev_out);
     if (p->gstream) cudaStreamDestroy(p->gstream);
 }
+
+// Buffers one call may touch, for the bounds-checking build (debug_bounds.cuh):
+// the plan's allocations and the caller's buffers, with their sizes.  In the
+// normal build every method is empty.
+struct BoundsScope {
+#ifdef RTM_BOUNDS_CHECK
+    std::vector<std::pair<unsigned long long, unsigned long long>> r;
+    void add(const void *ptr, size_t bytes) {
+        if (ptr && bytes) r.push_back({(unsigned long long)(uintptr_t)ptr, (unsigned long long)(uintptr_t)ptr + bytes});
+    }
+    int begin(cudaStream_t s) {
+        DbgTable t{};
+        if (r.size() > (size_t)DBG_MAX_RANGES) return fail(RTM_E_STATE, "bounds check: %zu buffers > %d", r.size(), DBG_MAX_RANGES);
+        for (size_t k = 0; k < r.size(); ++k) {
+            t.begin[k] = r[k].first;
+            t.end[k] = r[k].second;
+        }
+        t.n = (int)r.size();
+        const unsigned long long zero = 0;
+        CUDA_TRY(cudaMemcpyToSymbolAsync(g_dbg_table, &t, sizeof t, 0, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyToSymbolAsync(g_dbg_bad, &zero, sizeof zero, 0, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaStreamSynchronize(s));  // the table is a stack object's copy: upload before returning
+        return 0;
+    }
+    int end(cudaStream_t s) {
+        unsigned long long bad = 0, first = 0;
+        CUDA_TRY(cudaMemcpyFromSymbolAsync(&bad, g_dbg_bad, sizeof bad, 0, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyFromSymbolAsync(&first, g_dbg_first, sizeof first, 0, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        DbgTable none{};
+        CUDA_TRY(cudaMemcpyToSymbol(g_dbg_table, &none, sizeof none));  // later calls of other entry points: unchecked until set
+        if (bad) return fail(RTM_E_CUDA, "bounds check: %llu accesses outside every buffer (first at 0x%llx)", bad, first);
+        return 0;
+    }
+#else
+    void add(const void *, size_t) {}
+    int begin(cudaStream_t) { return 0; }
+    int end(cudaStream_t) { return 0; }
+#endif
+    void add_plan(const rtm_plan *p) {
+        const size_t F = sizeof(float);
+        add(p->d_shots, p->shots_h.size() * sizeof(ShotDev));
+        add(p->d_work, (size_t)p->n_work * sizeof(int4));
+        add(p->d_src_ptr, p->n_src_ptr * sizeof(int));
+        add(p->d_rec_ptr, p->n_rec_ptr * sizeof(int));
+        add(p->d_src_ent, p->n_src_ent * sizeof(int2));
+        add(p->d_rec_ent, p->n_rec_ent * sizeof(int2));
+        add(p->d_flags, p->nshots * sizeof(int));
+        add(p->d_fail_seq, p->nshots * sizeof(int));
+        add(p->d_sponge, (size_t)std::max(p->g.absorbing_frame, 1) * F);
+        for (int b = 0; b < 2; ++b)
+            for (int f = 0; f < NFIELD; ++f) add(p->d_state[b][f], p->state_floats * F);
+        const size_t mat = (size_t)(p->g.nx + 2) * p->pitch * F;
+        for (int m = 0; m < NMAT; ++m) add(p->d_mat[m], mat);
+        add(p->d_surface, mat);
+        for (int c = 0; c < 3; ++c) {
+            add(p->d_img[c], (size_t)p->rows_total * p->pitch * F);
+            add(p->d_imgc[c], (size_t)p->rows_total * p->pitch * F);
+        }
+        const size_t seis = std::max<size_t>((size_t)3 * p->g.nt * p->nrec_total, 1) * F;
+        add(p->d_seis_t, seis);
+        add(p->d_obs_t, seis);
+    }
+};
 
 // Run a time loop: directly on s, or (use_graphs) as a CUDA graph captured on
 // the plan's own stream the first time this key is seen and replayed after.
@@ -311,7 +384,37 @@ int zero_state(rtm_plan *p, cudaStream_t s) {
 
 extern "C" {
 
-const char *rtm_version(void) { return "rtm_b200 1.0 (sm_100a)"; }
+const char *rtm_version(void) {
+#ifdef RTM_BOUNDS_CHECK
+    return "rtm_b200 1.0 (sm_100a, bounds-checking build)";
+#else
+    return "rtm_b200 1.0 (sm_100a)";
+#endif
+}
+
+int rtm_bounds_probe(const rtm_plan *p, const void *buf, size_t buf_bytes, const void *ptr, size_t bytes,
+                     int32_t *inside) {
+#ifdef RTM_BOUNDS_CHECK
+    if (!p || !inside) return fail(RTM_E_ARG, "null argument");
+    BoundsScope bs;
+    bs.add_plan(p);
+    bs.add(buf, buf_bytes);
+    if (int rc = bs.begin(0)) return rc;
+    bounds_probe_kernel<<<1, 1>>>(ptr, (unsigned)bytes);
+    CUDA_TRY(cudaGetLastError());
+    int v = 0;
+    CUDA_TRY(cudaMemcpyFromSymbol(&v, g_dbg_probe, sizeof v));
+    *inside = v;
+    const unsigned long long zero = 0;
+    CUDA_TRY(cudaMemcpyToSymbol(g_dbg_bad, &zero, sizeof zero));  // the probe's own count
+    DbgTable none{};
+    CUDA_TRY(cudaMemcpyToSymbol(g_dbg_table, &none, sizeof none));
+    return RTM_OK;
+#else
+    (void)p; (void)buf; (void)buf_bytes; (void)ptr; (void)bytes; (void)inside;
+    return fail(RTM_E_STATE, "rtm_bounds_probe needs the bounds-checking build (-DRTM_BOUNDS_CHECK)");
+#endif
+}
 const char *rtm_last_error(void) { return g_err.c_str(); }
 
 int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, const rtm_tune *tune,
@@ -441,6 +544,10 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
     rc |= dalloc(&p->d_rec_ptr, rec_ptr.size());
     rc |= dalloc(&p->d_src_ent, std::max<size_t>(src_ent.size(), 1));
     rc |= dalloc(&p->d_rec_ent, std::max<size_t>(rec_ent.size(), 1));
+    p->n_src_ptr = src_ptr.size();
+    p->n_rec_ptr = rec_ptr.size();
+    p->n_src_ent = std::max<size_t>(src_ent.size(), 1);
+    p->n_rec_ent = std::max<size_t>(rec_ent.size(), 1);
     rc |= dalloc(&p->d_flags, nshots);
     rc |= dalloc(&p->d_fail_seq, nshots);
     rc |= dalloc(&p->d_sponge, std::max(g.absorbing_frame, 1));
@@ -509,6 +616,7 @@ long long rtm_plan_launch_count(const rtm_plan *p) { return p ? p->launches : 0;
 
 int rtm_plan_set_model(rtm_plan *p, const float *mu, const float *lam, const float *rho,
                        const float *surface, rtm_stream_t stream) {
+    NvtxRange nvtx_range("rtm_plan_set_model");
     if (!p || !mu || !lam || !rho) return fail(RTM_E_ARG, "null model pointer");
     cudaStream_t s = (cudaStream_t)stream;
     const size_t mat_floats = (size_t)(p->g.nx + 2) * p->pitch;
@@ -538,6 +646,7 @@ static int transpose(const float *in, float *out, int planes, int rows, int cols
 int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int isnap, float *snap_u,
                 float *snap_v, float *snap_w, int32_t *isnaps_out, int check_interval,
                 int32_t *flags, rtm_stream_t stream) {
+    NvtxRange nvtx_range("rtm_forward");
     if (!p) return fail(RTM_E_ARG, "null plan");
     if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
     if (p->nsrc_total > 0 && !wavelets) return fail(RTM_E_ARG, "null wavelets");
@@ -553,6 +662,13 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
                 return fail(RTM_E_ARG, "snapshot buffer %d is null", c);
     }
     cudaStream_t s = (cudaStream_t)stream;
+    BoundsScope bs;
+    bs.add_plan(p);
+    bs.add(wavelets, (size_t)3 * p->nsrc_total * nt * sizeof(float));
+    bs.add(seis, (size_t)3 * p->nrec_total * nt * sizeof(float));
+    if (save)
+        for (float *b : {snap_u, snap_v, snap_w}) bs.add(b, rtm_plan_snapshot_floats(p, nsnap) * sizeof(float));
+    if (int rc = bs.begin(s)) return rc;
     if (int rc = zero_state(p, s)) return rc;
     // Snapshot slots the time loop never reaches ((k+1)*isnap > nt-1) stay
     // zero, like the reference's zero-initialised fields (fm:533-535).
@@ -629,6 +745,7 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
         CUDA_TRY(cudaMemcpyAsync(flags, p->d_flags, p->nshots * sizeof(int), cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaStreamSynchronize(s));
     }
+    if (int rc = bs.end(s)) return rc;
     return RTM_OK;
 }
 
@@ -638,6 +755,7 @@ static int backward_impl(rtm_plan *p, const float *obs, const float *snap_u, con
                          const float *snap_w, const int32_t *isnaps, int num_snaps, int isnap, float *image,
                          double *stack, int check_interval, int32_t *flags, rtm_stream_t stream,
                          double norm_eps) {
+    NvtxRange nvtx_range("rtm_backward");
     if (!p) return fail(RTM_E_ARG, "null plan");
     if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
     if (p->nrec_total > 0 && !obs) return fail(RTM_E_ARG, "null observed data");
@@ -651,6 +769,13 @@ static int backward_impl(rtm_plan *p, const float *obs, const float *snap_u, con
             return fail(RTM_E_ARG, "snapshot buffer %d is null", c);
     const int nt = p->g.nt;
     cudaStream_t s = (cudaStream_t)stream;
+    BoundsScope bs;
+    bs.add_plan(p);
+    bs.add(obs, (size_t)3 * p->nrec_total * nt * sizeof(float));
+    for (const float *b : sp3) bs.add(b, rtm_plan_snapshot_floats(p, num_snaps) * sizeof(float));
+    bs.add(image, (size_t)3 * p->g.nx * p->g.nz * sizeof(float));
+    bs.add(stack, (size_t)3 * p->g.nx * p->g.nz * sizeof(double));
+    if (int rc = bs.begin(s)) return rc;
     if (int rc = zero_state(p, s)) return rc;
     const size_t img_floats = (size_t)p->rows_total * p->pitch;
     for (int c = 0; c < 3; ++c)
@@ -770,6 +895,7 @@ static int backward_impl(rtm_plan *p, const float *obs, const float *snap_u, con
     }
     if (flags) CUDA_TRY(cudaMemcpyAsync(flags, p->d_flags, p->nshots * sizeof(int), cudaMemcpyDeviceToHost, s));
     if (flags || norm) CUDA_TRY(cudaStreamSynchronize(s));  // scratch is freed on return
+    if (int rc = bs.end(s)) return rc;
     return RTM_OK;
 }
 
@@ -880,6 +1006,7 @@ int segment_start(rtm_plan *p, const void *ckpt, int dtype, int sgi, float *zero
 
 int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, int ckpt_every, int ckpt_dtype,
                              void *ckpt, int check_interval, int32_t *flags, rtm_stream_t stream) {
+    NvtxRange nvtx_range("rtm_forward_checkpointed");
     if (!p) return fail(RTM_E_ARG, "null plan");
     if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
     if (p->g.modes != RTM_PSV) return fail(RTM_E_ARG, "checkpointed propagation supports the P-SV mode");
@@ -890,6 +1017,12 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
     const int nck = rtm_plan_num_checkpoints(p, ckpt_every);
     if (nck > 0 && !ckpt) return fail(RTM_E_ARG, "null checkpoint buffer");
     cudaStream_t s = (cudaStream_t)stream;
+    BoundsScope bs;
+    bs.add_plan(p);
+    bs.add(wavelets, (size_t)3 * p->nsrc_total * nt * sizeof(float));
+    bs.add(seis, (size_t)3 * p->nrec_total * nt * sizeof(float));
+    bs.add(ckpt, rtm_plan_checkpoint_bytes(p, ckpt_every, ckpt_dtype));
+    if (int rc = bs.begin(s)) return rc;
     if (int rc = zero_state(p, s)) return rc;
     if (nck > 0 && ckpt_dtype == RTM_CKPT_F32)
         CUDA_TRY(cudaMemsetAsync(ckpt, 0, rtm_plan_checkpoint_bytes(p, ckpt_every, ckpt_dtype), s));
@@ -947,11 +1080,13 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
         CUDA_TRY(cudaMemcpyAsync(flags, p->d_flags, p->nshots * sizeof(int), cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaStreamSynchronize(s));
     }
+    if (int rc = bs.end(s)) return rc;
     return RTM_OK;
 }
 
 int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt_every, int ckpt_dtype,
                 const void *ckpt, double *grad, float *grad_wavelet, rtm_stream_t stream) {
+    NvtxRange nvtx_range("rtm_adjoint");
     if (!p) return fail(RTM_E_ARG, "null plan");
     if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
     if (p->g.modes != RTM_PSV) return fail(RTM_E_ARG, "the adjoint supports the P-SV mode");
@@ -985,7 +1120,15 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
         cleanup();
         return rc;
     }
+    BoundsScope bs;
+    bs.add_plan(p);
+    bs.add(wavelets, (size_t)3 * p->nsrc_total * nt * sizeof(float));
+    bs.add(ckpt, rtm_plan_checkpoint_bytes(p, ckpt_every, ckpt_dtype));
+    bs.add(seg, nslots * slot * sizeof(float));
+    bs.add(gsum, (size_t)3 * NGRAD * gfl * sizeof(float));
+    bs.add(gwt, (size_t)3 * nt * p->nsrc_total * sizeof(float));
     auto body = [&]() -> int {
+        if (int r = bs.begin(s)) return r;
         CUDA_TRY(cudaMemsetAsync(p->d_flags, 0, p->nshots * sizeof(int), s));
         CUDA_TRY(cudaMemsetAsync(p->d_fail_seq, 0x7f, p->nshots * sizeof(int), s));
         CUDA_TRY(cudaMemsetAsync(seg, 0, nslots * slot * sizeof(float), s));
@@ -1105,6 +1248,7 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
             if (int r = transpose(gwt, grad_wavelet, 3, nt, p->nsrc_total, s)) return r;
         }
         CUDA_TRY(cudaStreamSynchronize(s));
+        if (int r = bs.end(s)) return r;
         return RTM_OK;
     };
     rc = body();
@@ -1115,6 +1259,7 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
 int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *obs, int ckpt_every,
                               int ckpt_dtype, const void *ckpt, int isnap, float *image, double *stack,
                               int check_interval, int32_t *flags, rtm_stream_t stream) {
+    NvtxRange nvtx_range("rtm_backward_checkpointed");
     if (!p) return fail(RTM_E_ARG, "null plan");
     if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
     if (p->g.modes != RTM_PSV) return fail(RTM_E_ARG, "checkpointed RTM supports the P-SV mode");
@@ -1137,7 +1282,16 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
     float *buf = nullptr;
     const size_t nbuf = 4 * slot + 2 * snap_comp;
     if (int rc = dalloc(&buf, nbuf)) return rc;
+    BoundsScope bs;
+    bs.add_plan(p);
+    bs.add(wavelets, (size_t)3 * p->nsrc_total * nt * sizeof(float));
+    bs.add(obs, (size_t)3 * p->nrec_total * nt * sizeof(float));
+    bs.add(ckpt, rtm_plan_checkpoint_bytes(p, ckpt_every, ckpt_dtype));
+    bs.add(image, (size_t)3 * p->g.nx * p->g.nz * sizeof(float));
+    bs.add(stack, (size_t)3 * p->g.nx * p->g.nz * sizeof(double));
+    bs.add(buf, nbuf * sizeof(float));
     auto body = [&]() -> int {
+        if (int rc = bs.begin(s)) return rc;
         if (int rc = zero_state(p, s)) return rc;
         CUDA_TRY(cudaMemsetAsync(buf, 0, nbuf * sizeof(float), s));
         const size_t img_floats = (size_t)p->rows_total * p->pitch;
@@ -1258,6 +1412,7 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
         }
         if (flags) CUDA_TRY(cudaMemcpyAsync(flags, p->d_flags, p->nshots * sizeof(int), cudaMemcpyDeviceToHost, s));
         CUDA_TRY(cudaStreamSynchronize(s));
+        if (int rc = bs.end(s)) return rc;
         return RTM_OK;
     };
     const int rc = body();

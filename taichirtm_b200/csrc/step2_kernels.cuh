@@ -61,6 +61,11 @@ __device__ __forceinline__ void copy_arr(float (&d)[VEC], const float (&s)[VEC])
 // imaging), which the read-only path (ld.global.nc) does not allow.
 template <int VEC>
 __device__ __forceinline__ void ldv_coherent(float (&v)[VEC], float *p) {
+    if (!RTM_DBG_OK(p, VEC * sizeof(float))) {
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) v[q] = 0.f;
+        return;
+    }
     if constexpr (VEC == 4) {
         const float4 t = *reinterpret_cast<float4 *>(p);
         v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
@@ -300,9 +305,9 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
         if (r < 0 || r >= nx) return;
         if constexpr (DIR == 0) {
             if (no_src) return;
-            const int e0 = __ldg(p.src_ptr + sh.src_row0 + r), e1 = __ldg(p.src_ptr + sh.src_row0 + r + 1);
+            const int e0 = ldg_chk(p.src_ptr + sh.src_row0 + r), e1 = ldg_chk(p.src_ptr + sh.src_row0 + r + 1);
             for (int e = e0; e < e1; ++e) {
-                const int2 en = __ldg(p.src_ent + e);
+                const int2 en = ldg_chk(p.src_ent + e);
                 const int q = en.x - c0;
                 if (q < 0 || q >= VEC) continue;
                 const bool in = interior(r, en.x, nx, nz);
@@ -312,17 +317,17 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
                 for (int qq = 0; qq < VEC; ++qq) {
                     if (qq != q) continue;
                     if constexpr (PSV) {
-                        out.u[qq] += __ldg(p.wav[0] + ti) * f * (in ? ir.u[qq] : __int_as_float(0x7f800000));
-                        out.w[qq] += __ldg(p.wav[2] + ti) * f * (in ? ir.w[qq] : __int_as_float(0x7f800000));
+                        out.u[qq] += ldg_chk(p.wav[0] + ti) * f * (in ? ir.u[qq] : __int_as_float(0x7f800000));
+                        out.w[qq] += ldg_chk(p.wav[2] + ti) * f * (in ? ir.w[qq] : __int_as_float(0x7f800000));
                     }
-                    if constexpr (SH) out.v[qq] += __ldg(p.wav[1] + ti) * f * ir.v[qq];
+                    if constexpr (SH) out.v[qq] += ldg_chk(p.wav[1] + ti) * f * ir.v[qq];
                 }
             }
         } else {
             if (no_rec) return;
-            const int e0 = __ldg(p.rec_ptr + sh.rec_row0 + r), e1 = __ldg(p.rec_ptr + sh.rec_row0 + r + 1);
+            const int e0 = ldg_chk(p.rec_ptr + sh.rec_row0 + r), e1 = ldg_chk(p.rec_ptr + sh.rec_row0 + r + 1);
             for (int e = e0; e < e1; ++e) {
-                const int2 en = __ldg(p.rec_ent + e);
+                const int2 en = ldg_chk(p.rec_ent + e);
                 const int q = en.x - c0;
                 if (q < 0 || q >= VEC) continue;
                 const size_t ti = (size_t)t * p.nrec_total + en.y;
@@ -330,10 +335,10 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
                 for (int qq = 0; qq < VEC; ++qq) {
                     if (qq != q) continue;
                     if constexpr (PSV) {
-                        out.u[qq] += __ldg(p.obs[0] + ti);
-                        out.w[qq] += __ldg(p.obs[2] + ti);
+                        out.u[qq] += ldg_chk(p.obs[0] + ti);
+                        out.w[qq] += ldg_chk(p.obs[2] + ti);
                     }
-                    if constexpr (SH) out.v[qq] += __ldg(p.obs[1] + ti);
+                    if constexpr (SH) out.v[qq] += ldg_chk(p.obs[1] + ti);
                 }
             }
         }
@@ -438,18 +443,18 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     // Kahan imaging against snapshot slot k.
     auto epilogue = [&](int r, int t, int k, const Vel &v) {
         if constexpr (DIR == 0) {
-            const int e0 = no_rec ? 0 : __ldg(p.rec_ptr + sh.rec_row0 + r);
-            const int e1 = no_rec ? 0 : __ldg(p.rec_ptr + sh.rec_row0 + r + 1);
+            const int e0 = no_rec ? 0 : ldg_chk(p.rec_ptr + sh.rec_row0 + r);
+            const int e1 = no_rec ? 0 : ldg_chk(p.rec_ptr + sh.rec_row0 + r + 1);
             for (int e = e0; e < e1; ++e) {
-                const int2 en = __ldg(p.rec_ent + e);
+                const int2 en = ldg_chk(p.rec_ent + e);
                 const int q = en.x - c0;
                 if (q < 0 || q >= VEC) continue;
                 const size_t ti = (size_t)t * p.nrec_total + en.y;
 #pragma unroll
                 for (int qq = 0; qq < VEC; ++qq) {
                     if (qq != q) continue;
-                    if constexpr (PSV) { p.seis[0][ti] = v.u[qq]; p.seis[2][ti] = v.w[qq]; }
-                    if constexpr (SH) p.seis[1][ti] = v.v[qq];
+                    if constexpr (PSV) { st_chk(p.seis[0] + ti, v.u[qq]); st_chk(p.seis[2] + ti, v.w[qq]); }
+                    if constexpr (SH) st_chk(p.seis[1] + ti, v.v[qq]);
                 }
             }
             if (k >= 0) {

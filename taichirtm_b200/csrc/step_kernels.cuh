@@ -41,6 +41,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "debug_bounds.cuh"
+
 namespace rtm {
 
 constexpr int COL_OFF = 4;
@@ -92,18 +94,19 @@ struct StepParams {
 template <int VEC>
 __device__ __forceinline__ void ldv(float (&v)[VEC], const float *__restrict__ p) {
     if constexpr (VEC == 4) {
-        float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+        float4 t = ldg_chk(reinterpret_cast<const float4 *>(p));
         v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
     } else if constexpr (VEC == 2) {
-        float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+        float2 t = ldg_chk(reinterpret_cast<const float2 *>(p));
         v[0] = t.x; v[1] = t.y;
     } else {
-        v[0] = __ldg(p);
+        v[0] = ldg_chk(p);
     }
 }
 
 template <int VEC>
 __device__ __forceinline__ void stv(float *__restrict__ p, const float (&v)[VEC]) {
+    if (!RTM_DBG_OK(p, VEC * sizeof(float))) return;
     if constexpr (VEC == 4) {
         *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
     } else if constexpr (VEC == 2) {
@@ -129,6 +132,11 @@ __device__ __forceinline__ unsigned long long l2_policy_evict_last() {
 // Read-only vector load with an L2 cache policy.
 template <int VEC>
 __device__ __forceinline__ void ldv_pol(float (&v)[VEC], const float *__restrict__ p, unsigned long long pol) {
+    if (!RTM_DBG_OK(p, VEC * sizeof(float))) {
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) v[q] = 0.f;
+        return;
+    }
     if constexpr (VEC == 4) {
         asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
             : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
@@ -143,6 +151,7 @@ __device__ __forceinline__ void ldv_pol(float (&v)[VEC], const float *__restrict
 // Vector store with an L2 cache policy.
 template <int VEC>
 __device__ __forceinline__ void stv_pol(float *p, const float (&v)[VEC], unsigned long long pol) {
+    if (!RTM_DBG_OK(p, VEC * sizeof(float))) return;
     if constexpr (VEC == 4) {
         asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;"
                      :: "l"(p), "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "l"(pol) : "memory");
@@ -158,6 +167,7 @@ __device__ __forceinline__ void stv_pol(float *p, const float (&v)[VEC], unsigne
 // completion tracked per thread by commit / wait groups: no spinning).
 template <int VEC>
 __device__ __forceinline__ void cp_async_vec(float *smem, const float *gmem) {
+    if (!RTM_DBG_OK(gmem, VEC * sizeof(float))) return;
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     if constexpr (VEC == 4) {
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
@@ -190,7 +200,7 @@ __device__ __forceinline__ float sponge_coef(const StepParams &p, int nx, int i,
     if (i >= 0 && i < fw && db > i) d = i;
     if (dr >= 0 && dr < fw && db > dr) d = dr;
     if (db >= 0 && db < fw && i >= db && dr >= db) d = db;
-    return d >= 0 ? __ldg(p.sponge + d) : 1.0f;
+    return d >= 0 ? ldg_chk(p.sponge + d) : 1.0f;
 }
 
 __device__ __forceinline__ bool interior(int i, int j, int nx, int nz) {
@@ -202,12 +212,14 @@ __device__ __forceinline__ bool interior(int i, int j, int nx, int nz) {
 // row is updated, recorded and imaged at the failing step, as the reference
 // does before it returns (forward_modeling.py:562-566).
 __device__ __forceinline__ bool shot_stopped(const StepParams &p, int shot) {
-    return p.fail_seq ? p.fail_seq[shot] < p.seq : __ldg(p.flags + shot) != 0;
+    if (p.fail_seq && !RTM_DBG_OK(p.fail_seq + shot, sizeof(int))) return true;
+    return p.fail_seq ? p.fail_seq[shot] < p.seq : ldg_chk(p.flags + shot) != 0;
 }
 
 // Record a failed check of this launch: the highest code wins, the first
 // failing launch stops the shot for the launches after it.
 __device__ __forceinline__ void report_failure(const StepParams &p, int shot, int code) {
+    if (!RTM_DBG_OK(p.flags + shot, sizeof(int)) || (p.fail_seq && !RTM_DBG_OK(p.fail_seq + shot, sizeof(int)))) return;
     atomicMax(p.flags + shot, code);
     if (p.fail_seq) atomicMin(p.fail_seq + shot, p.seq);
 }
@@ -365,9 +377,9 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
         if (i < 0 || i >= nx) return;
         if ((DIR == 0 && no_src) || (DIR == 1 && no_rec)) return;
         if constexpr (DIR == 0) {
-            const int e0 = __ldg(p.src_ptr + sh.src_row0 + i), e1 = __ldg(p.src_ptr + sh.src_row0 + i + 1);
+            const int e0 = ldg_chk(p.src_ptr + sh.src_row0 + i), e1 = ldg_chk(p.src_ptr + sh.src_row0 + i + 1);
             for (int e = e0; e < e1; ++e) {
-                const int2 en = __ldg(p.src_ent + e);
+                const int2 en = ldg_chk(p.src_ent + e);
                 const int q = en.x - c0;
                 if (q < 0 || q >= VEC) continue;
                 const bool in = interior(i, en.x, nx, nz);
@@ -377,16 +389,16 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
                 for (int qq = 0; qq < VEC; ++qq) {
                     if (qq != q) continue;
                     if constexpr (PSV) {
-                        u_c[qq] += __ldg(p.wav[0] + t) * f * (in ? ir_u[qq] : __int_as_float(0x7f800000));
-                        w_c[qq] += __ldg(p.wav[2] + t) * f * (in ? ir_w[qq] : __int_as_float(0x7f800000));
+                        u_c[qq] += ldg_chk(p.wav[0] + t) * f * (in ? ir_u[qq] : __int_as_float(0x7f800000));
+                        w_c[qq] += ldg_chk(p.wav[2] + t) * f * (in ? ir_w[qq] : __int_as_float(0x7f800000));
                     }
-                    if constexpr (SH) v_c[qq] += __ldg(p.wav[1] + t) * f * ir_v[qq];
+                    if constexpr (SH) v_c[qq] += ldg_chk(p.wav[1] + t) * f * ir_v[qq];
                 }
             }
         } else {
-            const int e0 = __ldg(p.rec_ptr + sh.rec_row0 + i), e1 = __ldg(p.rec_ptr + sh.rec_row0 + i + 1);
+            const int e0 = ldg_chk(p.rec_ptr + sh.rec_row0 + i), e1 = ldg_chk(p.rec_ptr + sh.rec_row0 + i + 1);
             for (int e = e0; e < e1; ++e) {
-                const int2 en = __ldg(p.rec_ent + e);
+                const int2 en = ldg_chk(p.rec_ent + e);
                 const int q = en.x - c0;
                 if (q < 0 || q >= VEC) continue;
                 const size_t t = (size_t)p.it * p.nrec_total + en.y;
@@ -394,10 +406,10 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
                 for (int qq = 0; qq < VEC; ++qq) {
                     if (qq != q) continue;
                     if constexpr (PSV) {
-                        u_c[qq] += __ldg(p.obs[0] + t);
-                        w_c[qq] += __ldg(p.obs[2] + t);
+                        u_c[qq] += ldg_chk(p.obs[0] + t);
+                        w_c[qq] += ldg_chk(p.obs[2] + t);
                     }
-                    if constexpr (SH) v_c[qq] += __ldg(p.obs[1] + t);
+                    if constexpr (SH) v_c[qq] += ldg_chk(p.obs[1] + t);
                 }
             }
         }
@@ -494,18 +506,18 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
         }
         if constexpr (DIR == 0) {
             // _record_seismogram_kernel (forward_modeling.py:445-453)
-            const int e0 = no_rec ? 0 : __ldg(p.rec_ptr + sh.rec_row0 + r);
-            const int e1 = no_rec ? 0 : __ldg(p.rec_ptr + sh.rec_row0 + r + 1);
+            const int e0 = no_rec ? 0 : ldg_chk(p.rec_ptr + sh.rec_row0 + r);
+            const int e1 = no_rec ? 0 : ldg_chk(p.rec_ptr + sh.rec_row0 + r + 1);
             for (int e = e0; e < e1; ++e) {
-                const int2 en = __ldg(p.rec_ent + e);
+                const int2 en = ldg_chk(p.rec_ent + e);
                 const int q = en.x - c0;
                 if (q < 0 || q >= VEC) continue;
                 const size_t t = (size_t)p.it * p.nrec_total + en.y;
 #pragma unroll
                 for (int qq = 0; qq < VEC; ++qq) {
                     if (qq != q) continue;
-                    if constexpr (PSV) { p.seis[0][t] = o_u[qq]; p.seis[2][t] = o_w[qq]; }
-                    if constexpr (SH) p.seis[1][t] = o_v[qq];
+                    if constexpr (PSV) { st_chk(p.seis[0] + t, o_u[qq]); st_chk(p.seis[2] + t, o_w[qq]); }
+                    if constexpr (SH) st_chk(p.seis[1] + t, o_v[qq]);
                 }
             }
             // _save_snapshot_kernel (forward_modeling.py:490-497, 569-572)
