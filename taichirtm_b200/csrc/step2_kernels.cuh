@@ -16,8 +16,11 @@
 //   backward: A velocity k-1, A stress k-1, B velocity k-2, B stress k-2
 // and a task that writes rows [ia, ib) recomputes step A on one extra row
 // above and below (rows ia-1 .. ib) from the old state of rows ia-2 .. ib+1.
-// Rows -2 and nx+1 lie outside the padded shot block and read as zero; no
-// update touches a non-interior cell, so pad rows stay zero.
+// Row indices are clamped to the pad rows -1 .. nx of the shot block: rows -2
+// and nx+1 read the zero pad state (no update touches a non-interior cell, so
+// pad rows stay zero), and the material read there feeds only updates of
+// non-interior cells, which the interior selects discard.  The loads need no
+// per-row branch.
 //
 // Columns.  Lanes 0 and 31 carry VEC halo columns.  After step A only their
 // outermost column is wrong (its neighbour is outside the warp); after step
@@ -113,23 +116,22 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     const int c0 = j0 - VEC + VEC * lane;
     const bool owner = lane >= 1 && lane <= 30;
     const int ia = wk.z, ib = wk.w;
-    const bool lane_in = c0 >= 1 && c0 + VEC - 1 <= nz - 2;
-    const bool lane_far = nz - 1 - (c0 + VEC - 1) >= p.fw;
-    auto all_in = [&](int i) { return lane_in && i >= 1 && i <= nx - 2; };
-    auto all_far = [&](int i) { return lane_far && i >= p.fw && nx - 1 - i >= p.fw; };
+    // The fast paths are chosen per warp (one uniform branch): a warp whose
+    // columns are not all interior / outside the sponge runs the general path
+    // on every lane instead of both paths.
+    const bool strip_in = __all_sync(FULL, c0 >= 1 && c0 + VEC - 1 <= nz - 2);
+    const bool strip_far = __all_sync(FULL, nz - 1 - (c0 + VEC - 1) >= p.fw);
+    auto all_in = [&](int i) { return strip_in && i >= 1 && i <= nx - 2; };
+    auto all_far = [&](int i) { return strip_far && i >= p.fw && nx - 1 - i >= p.fw; };
     const long long soff = sh.state_off + (long long)(c0 + COL_OFF);
     const long long moff = (long long)sh.x0 * P + (long long)(c0 + COL_OFF);
     const float dt = p.dt, idx = p.inv_dx, idz = p.inv_dz;
     const float sdt = DIR == 0 ? dt : -dt;
     // rows -1 and nx are the zero pad rows of the shot block (and of the
-    // material window); rows beyond them are never read
-    auto row_ok = [&](int i) { return i >= -1 && i <= nx; };
-    auto LSt = [&](float (&v)[VEC], int f, int i) {
-        if (row_ok(i)) ldv<VEC>(v, p.sin[f] + soff + (long long)(i + 1) * P); else zero_arr<VEC>(v);
-    };
-    auto LMt = [&](float (&v)[VEC], int m, int i) {
-        if (row_ok(i)) ldv<VEC>(v, p.mat[m] + moff + (long long)(i + 1) * P); else zero_arr<VEC>(v);
-    };
+    // material window); rows beyond them read the pad row (header comment)
+    auto rowc = [&](int i) { return min(max(i, -1), nx); };
+    auto LSt = [&](float (&v)[VEC], int f, int i) { ldv<VEC>(v, p.sin[f] + soff + (long long)(rowc(i) + 1) * P); };
+    auto LMt = [&](float (&v)[VEC], int m, int i) { ldv<VEC>(v, p.mat[m] + moff + (long long)(rowc(i) + 1) * P); };
     auto load_sig = [&](int i, Sig &s) {
         if constexpr (PSV) { LSt(s.xx, F_SXX, i); LSt(s.zz, F_SZZ, i); LSt(s.xz, F_SXZ, i); }
         if constexpr (SH) { LSt(s.yx, F_SYX, i); LSt(s.yz, F_SYZ, i); }
@@ -146,7 +148,7 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
         if constexpr (PSV) { LMt(m.lam, M_LAM, i); LMt(m.mu, M_MU, i); LMt(m.mxz, M_MXZ, i); }
         if constexpr (SH) { LMt(m.myx, M_MYX, i); LMt(m.myz, M_MYZ, i); }
         if (p.surface) {
-            if (row_ok(i)) ldv<VEC>(m.sm, p.surface + moff + (long long)(i + 1) * P); else zero_arr<VEC>(m.sm);
+            ldv<VEC>(m.sm, p.surface + moff + (long long)(rowc(i) + 1) * P);
         } else {
 #pragma unroll
             for (int q = 0; q < VEC; ++q) m.sm[q] = 1.f;
@@ -165,13 +167,7 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     };
     auto ring_issue = [&](int row) {
         auto put = [&](int f, const float *src) {
-            if (row_ok(row)) {
-                cp_async_vec<VEC>(rslot(row, f), src + moff + (long long)(row + 1) * P);
-            } else {
-                float *d = rslot(row, f);
-#pragma unroll
-                for (int q = 0; q < VEC; ++q) d[q] = 0.f;  // rows beyond the pads read as zero
-            }
+            cp_async_vec<VEC>(rslot(row, f), src + moff + (long long)(rowc(row) + 1) * P);
         };
         if constexpr (PSV) {
             put(RF_LAM, p.mat[M_LAM]); put(RF_MU, p.mat[M_MU]); put(RF_MXZ, p.mat[M_MXZ]);
