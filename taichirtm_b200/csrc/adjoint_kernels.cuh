@@ -135,7 +135,8 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
     const int4 wk = p.work[task];
     const ShotDev sh = p.shots[wk.x];
     const int nx = sh.nx, nz = p.nz, P = p.pitch;
-    const int c0 = (wk.y & 0xFFFFF) * W - VEC + VEC * lane;  // bits 20+ are step-kernel hints
+    const int c0 = (wk.y & 0xFFFFF) * W - VEC + VEC * lane;
+    const bool no_src = (wk.y >> 20) & 1, no_rec = (wk.y >> 21) & 1;
     const bool owner = lane >= 1 && lane <= 30;
     const int ia = wk.z, ib = wk.w;
     const long long soff = sh.state_off + (long long)(c0 + COL_OFF);
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
                 gw[q] = in ? dt * bw[q] * aw[q] : 0.f;
             }
             // sources of row k: recompute injection (fm:421-443)
-            if (k < nx && n < p.nt) {
+            if (!no_src && k < nx && n < p.nt) {
                 const int e0 = ldg_chk(p.src_ptr + sh.src_row0 + k), e1 = ldg_chk(p.src_ptr + sh.src_row0 + k + 1);
                 for (int e = e0; e < e1; ++e) {
                     const int2 en = ldg_chk(p.src_ent + e);
@@ -327,8 +328,8 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
             }
             if (owner) {
                 // sources of row r: gradient of the injection scale and wavelet gradient
-                const int e0 = n < p.nt ? ldg_chk(p.src_ptr + sh.src_row0 + r) : 0;
-                const int e1 = n < p.nt ? ldg_chk(p.src_ptr + sh.src_row0 + r + 1) : 0;
+                const int e0 = !no_src && n < p.nt ? ldg_chk(p.src_ptr + sh.src_row0 + r) : 0;
+                const int e1 = !no_src && n < p.nt ? ldg_chk(p.src_ptr + sh.src_row0 + r + 1) : 0;
                 for (int e = e0; e < e1; ++e) {
                     const int2 en = ldg_chk(p.src_ent + e);
                     const int q = en.x - c0;
@@ -352,7 +353,7 @@ __global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
                     }
                 }
                 // R^T g_{n-1}: adjoint source at the receivers (fm:445-453 transposed)
-                if (n >= 1) {
+                if (!no_rec && n >= 1) {
                     const int e0r = ldg_chk(p.rec_ptr + sh.rec_row0 + r), e1r = ldg_chk(p.rec_ptr + sh.rec_row0 + r + 1);
                     for (int e = e0r; e < e1r; ++e) {
                         const int2 en = ldg_chk(p.rec_ent + e);
