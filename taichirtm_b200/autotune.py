@@ -50,9 +50,10 @@ def _store(cache):
     p = _cache_path()
     try:
         os.makedirs(os.path.dirname(p), exist_ok=True)
-        with open(p + ".tmp", "w") as f:
+        tmp = f"{p}.{os.getpid()}.tmp"  # one per process: ranks may store at the same time
+        with open(tmp, "w") as f:
             json.dump(cache, f, indent=1, sort_keys=True)
-        os.replace(p + ".tmp", p)
+        os.replace(tmp, p)
     except OSError:
         pass
 
