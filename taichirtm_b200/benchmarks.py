@@ -39,6 +39,37 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-300))
 
 
+def _plain_gradient(sv, shots, wav, obs, m0, K, nt, dev, nplain):
+    """The same gradient, one shot per problem (one shot per launch), each
+    problem with its own autotuned launch shape: shots/s over shots
+    0 .. nplain-1, each timed once after one untimed call."""
+    t_sum, shapes = 0.0, []
+    for s in range(nplain):
+        o0 = sum(len(x.src) for x in shots[:s])
+        r0 = sum(len(x.rec) for x in shots[:s])
+        w1 = wav[:, o0:o0 + len(shots[s].src)].contiguous()
+        ob1 = obs[:, r0:r0 + len(shots[s].rec)].contiguous()
+        one = FWIProblem(sv.nx, sv.nz, sv.dx, sv.dz, sv.fs, nt, sv.fw, [shots[s]], w1, ckpt_every=K,
+                         tune="auto", device=dev)
+        shapes.append(one.tune)
+
+        def grad1():
+            m = [x.clone().requires_grad_(True) for x in m0]
+            l2_misfit(m[0], m[1], m[2], one, ob1).backward()
+        grad1()
+        torch.cuda.synchronize()
+        a, b = _ev(), _ev()
+        a.record()
+        grad1()
+        b.record()
+        torch.cuda.synchronize()
+        t_sum += a.elapsed_time(b)
+        one.close()
+    return dict(shots_per_s=round(nplain / (t_sum / 1000.0), 3), launch_shapes=shapes,
+                sample=f"shots 0..{nplain - 1}, one shot per problem (one shot per launch), "
+                       "each with its own autotuned launch shape")
+
+
 def run_c4(args):
     nt = args.nt or 3000
     sv = S.config4(nt=nt)
@@ -73,6 +104,7 @@ def run_c4(args):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     cells = sum(s.nx for s in shots) * sv.nz
+    plain = _plain_gradient(sv, shots, wav, obs, m0, K, nt, dev, nplain=2)
     # reference backward + imaging (zero-lag cross-correlation) with the data
     # residual as "observed data": its image vs the exact gradient (reported)
     rtm = BatchedRTM(*sv.material(migration=True), sv.dx, sv.dz, sv.fs, nt, sv.fw, shots,
@@ -93,6 +125,7 @@ def run_c4(args):
                                                ckpt_every=K, checkpoint_gb=round(prob.checkpoint_bytes() / 1e9, 2),
                                                launch_shape=dict(rtm=tune, gradient=prob.tune)),
                 gcell_upd_per_s=round(2 * cells * nt / (ms / 1000.0) / 1e9, 2), misfit=J,
+                plain=plain, batched_vs_plain=round(len(shots) / (ms / 1000.0) / plain["shots_per_s"], 2),
                 normalized_corr_gradient_vs_reference_rtm_image=corr,
                 note="finite-difference (FP64, 10 directions) and dot-product checks: tests/test_gpu_adjoint.py")
     prob.close()
