@@ -90,6 +90,13 @@ struct rtm_plan {
     float *d_seis_t = nullptr, *d_obs_t = nullptr;
     int *d_flags = nullptr;
     int *d_fail_seq = nullptr;  // per shot: first failing launch of the current loop
+    // Scratch of the checkpointed entry points (rtm_adjoint,
+    // rtm_backward_checkpointed): kept and reused from call to call, grown
+    // when a call needs more, freed with the plan.  A cudaMalloc / cudaFree
+    // pair of several GB per call costs a device-wide synchronisation and
+    // page mapping on every gradient.
+    float *d_scratch = nullptr;
+    size_t scratch_floats = 0;
     bool model_set = false;
     long long launches = 0;
     // CUDA-graph replay of time loops (tune.graphs): one cached executable per
@@ -112,6 +119,19 @@ bool field_active(int modes, int f) {
 }
 bool comp_active(int modes, int c) { return c == 1 ? (modes & RTM_SH) : (modes & RTM_PSV); }
 
+// The plan's scratch, at least n floats (contents undefined).
+int plan_scratch(rtm_plan *p, size_t n, float **out) {
+    if (p->scratch_floats < n) {
+        if (p->d_scratch) cudaFree(p->d_scratch);
+        p->d_scratch = nullptr;
+        p->scratch_floats = 0;
+        if (int rc = dalloc(&p->d_scratch, n)) return rc;
+        p->scratch_floats = n;
+    }
+    *out = p->d_scratch;
+    return 0;
+}
+
 void plan_free(rtm_plan *p) {
     auto F = [](void *q) { if (q) cudaFree(q); };
     F(p->d_shots); F(p->d_work); F(p->d_src_ptr); F(p->d_rec_ptr); F(p->d_src_ent); F(p->d_rec_ent);
@@ -119,7 +139,7 @@ void plan_free(rtm_plan *p) {
     for (int m = 0; m < NMAT; ++m) F(p->d_mat[m]);
     F(p->d_surface); F(p->d_sponge);
     for (int c = 0; c < 3; ++c) { F(p->d_img[c]); F(p->d_imgc[c]); }
-    F(p->d_seis_t); F(p->d_obs_t); F(p->d_flags); F(p->d_fail_seq);
+    F(p->d_seis_t); F(p->d_obs_t); F(p->d_flags); F(p->d_fail_seq); F(p->d_scratch);
     for (auto *gc : {&p->g_fwd, &p->g_bwd, &p->g_ckpt})
         if (gc->exec) cudaGraphExecDestroy(gc->exec);
     if (p->ev_in) cudaEventDestroy(p->ev_in);
@@ -1105,21 +1125,15 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
     const size_t gfl = (size_t)p->rows_total * p->pitch;
     // scratch: K-1 recompute slots, zero state, 2 adjoint states, unpack stage;
     // Kahan gradients; wavelet gradient
-    float *seg = nullptr, *gsum = nullptr, *gwt = nullptr;
+    // (the plan's scratch, subdivided; every piece starts on a 128-byte
+    // boundary since state_floats and gfl are multiples of the pitch)
     const size_t nrec_slots = (size_t)std::max(K - 1, 1);
     const size_t nslots = nrec_slots + 1 + 2 + (ckpt_dtype == RTM_CKPT_F32 ? 0 : 1);
-    int rc = dalloc(&seg, nslots * slot);
-    if (!rc) rc = dalloc(&gsum, (size_t)3 * NGRAD * gfl);  // Kahan sums, compensations, partials
-    if (!rc && grad_wavelet && p->nsrc_total) rc = dalloc(&gwt, (size_t)3 * nt * p->nsrc_total);
-    auto cleanup = [&]() {
-        if (seg) cudaFree(seg);
-        if (gsum) cudaFree(gsum);
-        if (gwt) cudaFree(gwt);
-    };
-    if (rc) {
-        cleanup();
-        return rc;
-    }
+    const size_t n_gsum = (size_t)3 * NGRAD * gfl;  // Kahan sums, compensations, partials
+    const size_t n_gwt = grad_wavelet && p->nsrc_total ? (size_t)3 * nt * p->nsrc_total : 0;
+    float *scratch = nullptr;
+    if (int rc = plan_scratch(p, nslots * slot + n_gsum + n_gwt, &scratch)) return rc;
+    float *seg = scratch, *gsum = seg + nslots * slot, *gwt = n_gwt ? gsum + n_gsum : nullptr;
     BoundsScope bs;
     bs.add_plan(p);
     bs.add(wavelets, (size_t)3 * p->nsrc_total * nt * sizeof(float));
@@ -1251,9 +1265,7 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
         if (int r = bs.end(s)) return r;
         return RTM_OK;
     };
-    rc = body();
-    cleanup();
-    return rc;
+    return body();
 }
 
 int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *obs, int ckpt_every,
@@ -1281,7 +1293,7 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
     // scratch: recompute ping-pong (2 states), zero state, unpack stage, segment snapshots (u, w)
     float *buf = nullptr;
     const size_t nbuf = 4 * slot + 2 * snap_comp;
-    if (int rc = dalloc(&buf, nbuf)) return rc;
+    if (int rc = plan_scratch(p, nbuf, &buf)) return rc;
     BoundsScope bs;
     bs.add_plan(p);
     bs.add(wavelets, (size_t)3 * p->nsrc_total * nt * sizeof(float));
@@ -1415,9 +1427,7 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
         if (int rc = bs.end(s)) return rc;
         return RTM_OK;
     };
-    const int rc = body();
-    cudaFree(buf);
-    return rc;
+    return body();
 }
 
 }  // extern "C"

@@ -127,6 +127,26 @@ def test_checkpoint_interval_does_not_change_gradient():
     assert np.array_equal(out[0], out[1])
 
 
+def test_repeated_gradients_on_one_problem_are_identical():
+    """The adjoint's scratch (recompute slots, gradient sums) stays with the
+    plan from call to call and grows when a call needs more (here: the
+    wavelet gradient): every call starts from cleared scratch, so repeated
+    gradients are bit-identical."""
+    P = _problem(nt=200)
+    lam, mu, rho = (torch.as_tensor(x, dtype=torch.float32) for x in _lame(P["vp"], P["vs"], P["rho"]))
+    prob = _fwi(P, ckpt=11)
+    d, c, _ = prob.forward(lam, mu, rho)
+    g1, _ = prob.adjoint(d, c)
+    g2, gw = prob.adjoint(d, c, want_wavelet_grad=True)
+    g3, _ = prob.adjoint(d, c)
+    _, gw2 = prob.adjoint(d, c, want_wavelet_grad=True)
+    assert np.abs(g1.cpu().numpy()).max() > 0
+    assert np.array_equal(g1.cpu().numpy(), g2.cpu().numpy())
+    assert np.array_equal(g1.cpu().numpy(), g3.cpu().numpy())
+    assert np.array_equal(gw.cpu().numpy(), gw2.cpu().numpy())
+    prob.close()
+
+
 def test_windowed_shots_equal_cropped_standalone_runs():
     from taichirtm_b200.plan import Plan, ShotGeometry
     rng = np.random.default_rng(9)
