@@ -191,7 +191,10 @@ int rtm_forward_checkpointed(rtm_plan *plan, const float *wavelets, float *seis,
  * gradients dJ/d(lam, mu, mxz, inv_rho_u, inv_rho_w) into grad
  * ((5, nx, nz) float64, global grid; the caller zeroes it) and, if non-NULL,
  * writes dJ/d(wavelets) into grad_wavelet (3, nsrc_total, nt).  Image-style
- * Kahan FP32 accumulation per shot, FP64 sum over shots.  Synchronises. */
+ * Kahan FP32 accumulation per shot, FP64 sum over shots.  Synchronises.
+ * Its scratch (ckpt_every + 3 states plus the gradient sums) is allocated on
+ * the first call and kept by the plan, grown when a later call needs more,
+ * and freed by rtm_plan_destroy; rtm_backward_checkpointed shares it. */
 int rtm_adjoint(rtm_plan *plan, const float *wavelets, const float *resid, int ckpt_every,
                 int ckpt_dtype, const void *ckpt, double *grad, float *grad_wavelet,
                 rtm_stream_t stream);
