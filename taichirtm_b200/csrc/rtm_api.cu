@@ -306,7 +306,7 @@ cudaError_t launch_mode(const StepParams &sp, int modes, int vec, int warps, cud
     }
 }
 
-template <int DIR, int MODE, int VEC, bool RING>
+template <int DIR, int MODE, int VEC, bool RING, bool STOREA = false>
 cudaError_t launch_step2(const StepParams &sp, int warps, cudaStream_t s) {
     size_t smem = 0;
     if constexpr (RING) {
@@ -316,13 +316,13 @@ cudaError_t launch_step2(const StepParams &sp, int warps, cudaStream_t s) {
         static bool attr_set = false;  // per instantiation; raises the 48 KB default
         if (!attr_set) {
             const size_t want = std::min<size_t>(8 * ring2_smem_per_warp<MODE, VEC>(), kMaxSmem);
-            cudaError_t e = cudaFuncSetAttribute(step2_kernel<DIR, MODE, VEC, RING>,
+            cudaError_t e = cudaFuncSetAttribute(step2_kernel<DIR, MODE, VEC, RING, STOREA>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
             if (e != cudaSuccess) return e;
             attr_set = true;
         }
     }
-    step2_kernel<DIR, MODE, VEC, RING><<<(sp.n_work + warps - 1) / warps, 32 * warps, smem, s>>>(sp);
+    step2_kernel<DIR, MODE, VEC, RING, STOREA><<<(sp.n_work + warps - 1) / warps, 32 * warps, smem, s>>>(sp);
     return cudaGetLastError();
 }
 
@@ -330,6 +330,15 @@ template <int DIR, int MODE>
 cudaError_t launch_vec2(const StepParams &sp, int vec, bool ring, int warps, cudaStream_t s) {
     if (vec == 2) return ring ? launch_step2<DIR, MODE, 2, true>(sp, warps, s) : launch_step2<DIR, MODE, 2, false>(sp, warps, s);
     return ring ? launch_step2<DIR, MODE, 4, true>(sp, warps, s) : launch_step2<DIR, MODE, 4, false>(sp, warps, s);
+}
+
+// Forward recompute of the adjoint, P-SV: steps sp.it and sp.it2 in one
+// launch, storing the state after each (sp.souta, sp.sout).
+cudaError_t launch_recompute2(const StepParams &sp, int vec, int prefetch, int warps, cudaStream_t s) {
+    const bool ring = prefetch == 3;
+    if (vec == 2)
+        return ring ? launch_step2<0, RTM_PSV, 2, true, true>(sp, warps, s) : launch_step2<0, RTM_PSV, 2, false, true>(sp, warps, s);
+    return ring ? launch_step2<0, RTM_PSV, 4, true, true>(sp, warps, s) : launch_step2<0, RTM_PSV, 4, false, true>(sp, warps, s);
 }
 
 // Two steps (sp.it, sp.it2) in one launch; vec is 2 or 4 (checked at plan
@@ -1215,17 +1224,28 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
             const int start = sgi * K, end = std::min(start + K, nt);
             float *s0 = nullptr;
             if (int r = segment_start(p, ckpt, ckpt_dtype, sgi, zero, stage, &s0, s)) return r;
-            // recompute forward states start .. end-2 into seg slots 0 .. len-2
-            for (int it = start; it <= end - 2; ++it) {
+            // recompute forward states start .. end-2 into seg slots 0 .. len-2,
+            // two steps per launch (each state stored) where the plan runs two
+            for (int it = start; it <= end - 2;) {
                 float *src = it == start ? s0 : seg + (size_t)(it - 1 - start) * slot;
                 float *dst = seg + (size_t)(it - start) * slot;
+                const bool two = p->tsteps == 2 && p->vec >= 2 && it + 1 <= end - 2;
                 for (int f = 0; f < NADJ; ++f) {
                     sp.sin[f] = fld(src, f);
-                    sp.sout[f] = fld(dst, f);
+                    sp.souta[f] = two ? fld(dst, f) : nullptr;
+                    sp.sout[f] = two ? fld(dst + slot, f) : fld(dst, f);
                 }
                 sp.it = it;
                 sp.seq = it + 1;
-                CUDA_TRY((launch_mode<0>(sp, RTM_PSV, p->vec | (p->prefetch << 8), warps, s)));
+                if (two) {
+                    sp.it2 = it + 1;
+                    sp.snap_k2 = -1;
+                    CUDA_TRY(launch_recompute2(sp, p->vec, p->prefetch, warps, s));
+                    it += 2;
+                } else {
+                    CUDA_TRY((launch_mode<0>(sp, RTM_PSV, p->vec | (p->prefetch << 8), warps, s)));
+                    it += 1;
+                }
                 ++p->launches;
             }
             // reverse steps end-1 .. start

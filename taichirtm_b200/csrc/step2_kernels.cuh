@@ -95,9 +95,12 @@ __host__ __device__ constexpr size_t ring2_smem_per_warp() {
     return (size_t)RING2_ROWS * ring2_fields<MODE>() * 32 * VEC * sizeof(float);
 }
 
-template <int DIR, int MODE, int VEC, bool RING = false>
+// STOREA: also store step A's state (rows [ia, ib), into p.souta), for the
+// forward recompute of the FWI adjoint, which needs the state after every step.
+template <int DIR, int MODE, int VEC, bool RING = false, bool STOREA = false>
 __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     static_assert(VEC >= 2, "two steps per launch need two halo columns per side");
+    static_assert(!STOREA || DIR == 0, "only the forward recompute stores step A");
     constexpr bool PSV = (MODE & 1) != 0;
     constexpr bool SH = (MODE & 2) != 0;
     constexpr int W = 30 * VEC;
@@ -489,6 +492,23 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
             if constexpr (SH) code = max(code, bad_code(v.v[q], p.code_base + 1));
         }
     };
+    // step A's stress and absorbed velocity of row r (STOREA)
+    auto store_a = [&](int r, const Sig &os, const Vel &ov) {
+        const long long so = soff + (long long)(r + 1) * P;
+        if constexpr (PSV) {
+            stv<VEC>(p.souta[F_SXX] + so, os.xx);
+            stv<VEC>(p.souta[F_SZZ] + so, os.zz);
+            stv<VEC>(p.souta[F_SXZ] + so, os.xz);
+            stv<VEC>(p.souta[F_U] + so, ov.u);
+            stv<VEC>(p.souta[F_W] + so, ov.w);
+        }
+        if constexpr (SH) {
+            stv<VEC>(p.souta[F_SYX] + so, os.yx);
+            stv<VEC>(p.souta[F_SYZ] + so, os.yz);
+            stv<VEC>(p.souta[F_V] + so, ov.v);
+        }
+    };
+    (void)store_a;
     // step B's stress and absorbed velocity of row r: store, outputs, check
     auto finish_b = [&](int r, const Sig &os, const Vel &ov) {
         if (!owner) return;
@@ -544,7 +564,10 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
                     Mat m;
                     ring_mat(k - 1, m);
                     stress_update(k - 1, va_p, va_c, so_p, m, sa_c, vabs_c);
-                    if (owner && k - 1 >= ia && k - 1 < ib) epilogue(k - 1, tA, p.snap_k, vabs_c);
+                    if (owner && k - 1 >= ia && k - 1 < ib) {
+                        epilogue(k - 1, tA, p.snap_k, vabs_c);
+                        if constexpr (STOREA) store_a(k - 1, sa_c, vabs_c);
+                    }
                 }
                 if (k >= ia + 1) {
                     Vel ir;
@@ -637,7 +660,10 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
                 vel_update(k, tA, so_c, so_p, vo, ir_c, va_c);
                 if (k >= ia) {
                     stress_update(k - 1, va_p, va_c, so_p, m_c, sa_c, vabs_c);
-                    if (owner && k - 1 >= ia && k - 1 < ib) epilogue(k - 1, tA, p.snap_k, vabs_c);
+                    if (owner && k - 1 >= ia && k - 1 < ib) {
+                        epilogue(k - 1, tA, p.snap_k, vabs_c);
+                        if constexpr (STOREA) store_a(k - 1, sa_c, vabs_c);
+                    }
                 }
                 if (k >= ia + 1) vel_update(k - 1, tB, sa_c, sa_p, vabs_c, ir_p, vb_c);
                 if (k >= ia + 2) {

@@ -89,6 +89,7 @@ struct StepParams {
     int seq;                 // this launch's number in its time loop (increasing)
     int it;                  // forward: step it; backward: reversed time t
     int it2, snap_k2;        // two-step launches: time and snapshot slot of the second step
+    float *souta[NFIELD];    // two-step launches storing the first step's state too (recompute)
 };
 
 template <int VEC>
