@@ -27,6 +27,42 @@ def _ev():
     return torch.cuda.Event(enable_timing=True)
 
 
+_ROOT = __import__("os").path.dirname(__import__("os").path.dirname(__import__("os").path.abspath(__file__)))
+PEAK_FALLBACK_GBS = 6650.0
+STATE_BYTES_PER_CELL = 40     # P-SV state read + written once per time step, per shot cell
+MATERIAL_BYTES_PER_CELL = 20  # P-SV material read once per time step, per model cell under any window
+KAHAN_IMG_BYTES_PER_CELL = 32  # imaging step: Kahan sum/compensation RMW of u and w
+
+
+def _peak_hbm():
+    try:
+        with open(__import__("os").path.join(_ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return PEAK_FALLBACK_GBS, "fallback"
+
+
+def _union_cells(shots, nz):
+    rows = set()
+    for s in shots:
+        rows.update(range(s.x0, s.x0 + s.nx))
+    return len(rows) * nz
+
+
+def _step_bytes(shots, nz):
+    """Compulsory bytes of one P-SV time step of one phase for a batch: every
+    shot's state read and written once, the shared material read once."""
+    return STATE_BYTES_PER_CELL * sum(s.nx for s in shots) * nz + MATERIAL_BYTES_PER_CELL * _union_cells(shots, nz)
+
+
+def _roofline(nbytes, ms, model):
+    peak, kind = _peak_hbm()
+    achieved = nbytes / (ms / 1000.0) / 1e9
+    return dict(bound="hbm", achieved=round(achieved, 1), peak=peak, unit="GB/s", frac=round(achieved / peak, 4),
+                traffic=None, bytes_model=model, algorithmic_bytes=int(nbytes),
+                peak_source=kind + (" (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else ""))
+
+
 def _corr(a, b):
     a = np.asarray(a, np.float64).ravel()
     b = np.asarray(b, np.float64).ravel()
@@ -117,6 +153,10 @@ def run_c4(args):
     inner = (slice(sv.fw, sv.nx - sv.fw), slice(5, sv.nz - sv.fw))
     image_pm = img[0] + img[2]
     corr = {k: _corr(gk.cpu().numpy()[inner], image_pm[inner]) for k, gk in zip(("vp", "vs", "rho"), g)}
+    grad_bytes = 2 * nt * _step_bytes(shots, sv.nz) + 2 * prob.checkpoint_bytes()
+    roof = _roofline(grad_bytes, ms, "whole gradient of all shots: 2 phases x nt x (40 B per shot cell + 20 B per "
+                                     "model cell under any window) + checkpoints written and read once; the "
+                                     "recompute and the gradient sums are not counted; timed end to end per gradient")
     line = dict(metric="FWI gradient shots/s (P-SV, exact adjoint, sqrt(nt) FP32 checkpoints)",
                 value=round(len(shots) / (ms / 1000.0), 3), unit="shots/s", n_gpus=1, steps=args.steps,
                 warmup=args.warmup, ms_per_step=round(ms, 2), higher_is_better=True, dtype="f32",
@@ -124,7 +164,7 @@ def run_c4(args):
                                                         f"nt={nt}, L2 misfit on vx and vz, start = smoothed true model (sigma 15)",
                                                ckpt_every=K, checkpoint_gb=round(prob.checkpoint_bytes() / 1e9, 2),
                                                launch_shape=dict(rtm=tune, gradient=prob.tune)),
-                gcell_upd_per_s=round(2 * cells * nt / (ms / 1000.0) / 1e9, 2), misfit=J,
+                gcell_upd_per_s=round(2 * cells * nt / (ms / 1000.0) / 1e9, 2), roofline=roof, misfit=J,
                 plain=plain, batched_vs_plain=round(len(shots) / (ms / 1000.0) / plain["shots_per_s"], 2),
                 normalized_corr_gradient_vs_reference_rtm_image=corr,
                 note="finite-difference (FP64, 10 directions) and dot-product checks: tests/test_gpu_adjoint.py")
@@ -147,6 +187,7 @@ def run_c5(args):
     stack = torch.zeros((3, sv.nx, sv.nz), dtype=torch.float64, device=dev)
     grad = None
     t_rtm = t_grad = 0.0
+    rtm_bytes = grad_bytes = 0
     peak_mem = 0
     errs = {}
     tune = None
@@ -170,6 +211,10 @@ def run_c5(args):
         torch.cuda.synchronize()
         t_rtm += a.elapsed_time(b)
         assert int(ff.max()) == 0 and int(fb.max()) == 0
+        shot_cells = sum(s.nx for s in shots) * sv.nz
+        n_img = sum(1 for t in range(1, nt) if t % isnap == 0 and t // isnap - 1 < nt // isnap)
+        ck_bytes = 2 * 5 * shot_cells * (nt // K)  # FP16 checkpoints, 5 fields
+        rtm_bytes += 2 * nt * _step_bytes(shots, sv.nz) + 2 * ck_bytes + n_img * KAHAN_IMG_BYTES_PER_CELL * shot_cells
         _, syn, _, _ = rtm.forward(wav)
         resid = (syn - obs)
         rtm.close()
@@ -182,6 +227,7 @@ def run_c5(args):
         b.record()
         torch.cuda.synchronize()
         t_grad += a.elapsed_time(b)
+        grad_bytes += 2 * nt * _step_bytes(shots, sv.nz) + 2 * prob.checkpoint_bytes()
         grad_tune = prob.tune
         grad = g if grad is None else grad + g
         del ck
@@ -219,6 +265,14 @@ def run_c5(args):
                             launch_shape=dict(rtm=tune, gradient=grad_tune)),
                 rtm_shots_per_s=round(n / (t_rtm / 1000), 4), gradient_shots_per_s=round(n / (t_grad / 1000), 4),
                 rtm_gcell_upd_per_s=round(2 * cells * nt / (t_rtm / 1000) / 1e9, 2),
+                roofline=dict(rtm=_roofline(rtm_bytes, t_rtm, "checkpointed RTM of all waves: 2 phases x nt x (40 B per "
+                                                                "shot cell + 20 B per model cell under any window) + FP16 "
+                                                                "checkpoints written and read once + 32 B per shot cell per "
+                                                                "imaging step (Kahan image RMW); recompute not counted"),
+                              gradient=_roofline(grad_bytes, t_grad, "gradient of all waves: 2 phases x nt x (40 B per "
+                                                                      "shot cell + 20 B per model cell under any window) "
+                                                                      "+ checkpoints written and read once; recompute and "
+                                                                      "gradient sums not counted")),
                 peak_device_memory_gb=round(peak_mem / 1e9, 1), errors=errs,
                 stack_finite=bool(torch.isfinite(stack).all()), grad_finite=bool(torch.isfinite(grad).all()),
                 note="FP32-stencil error against FP64 runs is measured by the parity tests; here the FP16 "
