@@ -30,6 +30,8 @@ CANDIDATES = [
     # small grids (one shot of a few hundred thousand cells): a warp's row loop
     # is a serial chain of dependent loads, so shorter tasks and more warps
     dict(vec=2, rows=2, warps=4, tsteps=2), dict(vec=2, rows=1, warps=4, tsteps=2),
+    dict(vec=2, rows=1, warps=1, tsteps=2), dict(vec=2, rows=1, warps=2, tsteps=2),
+    dict(vec=2, rows=2, warps=2, tsteps=2),
     dict(vec=1, rows=2, warps=4, prefetch=1), dict(vec=1, rows=1, warps=4, prefetch=1),
     dict(vec=2, rows=2, warps=4, prefetch=1),
 ]
@@ -66,7 +68,7 @@ def _store(cache):
 def key(nz, shots, modes):
     name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
     rows = sum(s.nx for s in shots)
-    return f"{name}|nz={nz}|rows={rows}|shots={len(shots)}|modes={modes}|v5"
+    return f"{name}|nz={nz}|rows={rows}|shots={len(shots)}|modes={modes}|v6"
 
 
 def time_shape(make_plan, shots, tune, steps=TUNE_STEPS):
