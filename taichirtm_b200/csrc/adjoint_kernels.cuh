@@ -45,6 +45,7 @@ struct AdjParams {
     int n_work;
     const ShotDev *shots;
     const float *fwd[NADJ];   // forward state n-1 (stored, absorbed): u, w, sxx, szz, sxz
+    const float *fwd2[NADJ];  // forward state n-2 (adjoint2_kernel: the second step reversed)
     const float *ain[NADJ];   // adjoint state n
     float *aout[NADJ];        // adjoint state n-1
     const float *mat[NMAT];

@@ -17,6 +17,7 @@
 #include "checkpoint_kernels.cuh"
 #include "aux_kernels.cuh"
 #include "step2_kernels.cuh"
+#include "adjoint2_kernels.cuh"
 #include "step_kernels.cuh"
 
 using namespace rtm;
@@ -1248,15 +1249,33 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
                 }
                 ++p->launches;
             }
-            // reverse steps end-1 .. start
-            for (int n = end - 1; n >= start; --n) {
-                float *fs = n == start ? s0 : seg + (size_t)(n - 1 - start) * slot;
+            // reverse steps end-1 .. start; with two steps per launch, steps n and
+            // n-1 together unless the partials are folded after step n
+            auto fwd_state = [&](int m) { return m == start ? s0 : seg + (size_t)(m - 1 - start) * slot; };
+            for (int n = end - 1; n >= start;) {
+                float *fs = fwd_state(n);
                 for (int f = 0; f < NADJ; ++f) {
                     ap.fwd[f] = fld(fs, f);
                     ap.ain[f] = fld(adj[cur], f);
                     ap.aout[f] = fld(adj[1 - cur], f);
                 }
                 ap.n = n;
+                if (p->tsteps == 2 && p->vec >= 2 && n - 1 >= start && n % GRAD_FOLD_STEPS != 0) {
+                    float *fs2 = fwd_state(n - 1);
+                    for (int f = 0; f < NADJ; ++f) ap.fwd2[f] = fld(fs2, f);
+                    if (p->vec == 2) adjoint2_kernel<2><<<blocks, 32 * warps, 0, s>>>(ap);
+                    else adjoint2_kernel<4><<<blocks, 32 * warps, 0, s>>>(ap);
+                    CUDA_TRY(cudaGetLastError());
+                    ++p->launches;
+                    cur = 1 - cur;
+                    n -= 2;
+                    if ((n + 1) % GRAD_FOLD_STEPS == 0) {  // after step n+1 (the pair's second)
+                        grad_fold_kernel<<<148 * 8, 256, 0, s>>>(fold);
+                        CUDA_TRY(cudaGetLastError());
+                        ++p->launches;
+                    }
+                    continue;
+                }
                 switch (p->vec) {
                     case 1: adjoint_step_kernel<1><<<blocks, 32 * warps, 0, s>>>(ap); break;
                     case 2: adjoint_step_kernel<2><<<blocks, 32 * warps, 0, s>>>(ap); break;
@@ -1270,6 +1289,7 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
                     CUDA_TRY(cudaGetLastError());
                     ++p->launches;
                 }
+                --n;
             }
         }
         const size_t n2 = (size_t)p->g.nx * p->g.nz;
