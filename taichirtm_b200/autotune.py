@@ -68,7 +68,7 @@ def _store(cache):
 def key(nz, shots, modes):
     name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
     rows = sum(s.nx for s in shots)
-    return f"{name}|nz={nz}|rows={rows}|shots={len(shots)}|modes={modes}|v6"
+    return f"{name}|nz={nz}|rows={rows}|shots={len(shots)}|modes={modes}|v7"
 
 
 def time_shape(make_plan, shots, tune, steps=TUNE_STEPS):
@@ -120,7 +120,8 @@ def best_shape(make_plan, nz, shots, modes, nt, candidates=None, refresh=False):
 # FWI gradients: the exact adjoint kernel dominates and prefers more, smaller
 # warp tasks than the forward step, so FWIProblem(tune="auto") times the
 # gradient itself (checkpointed forward + adjoint sweep) on a short time axis.
-FWI_CANDIDATES = [dict(vec=2, rows=r, warps=w, tsteps=2) for r in (4, 8, 16) for w in (1, 2, 4)]
+FWI_CANDIDATES = ([dict(vec=2, rows=r, warps=w, tsteps=2) for r in (4, 8, 16) for w in (1, 2, 4)]
+                  + [dict(vec=2, rows=32, warps=w, tsteps=2) for w in (1, 2)])
 FWI_TUNE_STEPS = 160
 
 
