@@ -192,6 +192,8 @@ int rtm_forward_checkpointed(rtm_plan *plan, const float *wavelets, float *seis,
  * ((5, nx, nz) float64, global grid; the caller zeroes it) and, if non-NULL,
  * writes dJ/d(wavelets) into grad_wavelet (3, nsrc_total, nt).  Image-style
  * Kahan FP32 accumulation per shot, FP64 sum over shots.  Synchronises.
+ * With two steps per launch (rtm_tune.tsteps 2) the segment recompute and
+ * the reverse sweep run steps in pairs; the gradient is bit-identical.
  * Its scratch (ckpt_every + 3 states plus the gradient sums) is allocated on
  * the first call and kept by the plan, grown when a later call needs more,
  * and freed by rtm_plan_destroy; rtm_backward_checkpointed shares it. */
