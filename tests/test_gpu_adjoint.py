@@ -147,6 +147,30 @@ def test_repeated_gradients_on_one_problem_are_identical():
     prob.close()
 
 
+def test_two_steps_per_launch_adjoint_is_taken_and_equal():
+    """With two steps per launch the segment recompute and the reverse sweep
+    run in pairs (about half the launches of one step per launch, not a
+    silent fallback), and the gradient is bit-identical."""
+    P = _problem(nt=200)
+    lam, mu, rho = _lame(P["vp"], P["vs"], P["rho"])
+    from taichirtm_b200.fwi import FWIProblem
+    from taichirtm_b200.plan import ShotGeometry
+    out = {}
+    for ts in (1, 2):
+        prob = FWIProblem(P["nx"], P["nz"], P["dx"], P["dz"], P["fs"], P["nt"], P["fw"],
+                          [ShotGeometry(0, P["nx"], P["src"], P["rec"])], P["wav"], ckpt_every=15,
+                          tune=dict(vec=2, rows=8, warps=2, tsteps=ts))
+        seis, ck, _ = prob.forward(lam, mu, rho)
+        g, _ = prob.adjoint(seis * 0.3, ck)
+        out[ts] = (g.cpu().numpy(), prob.plan.launch_count())
+        prob.close()
+    assert np.abs(out[1][0]).max() > 0
+    assert np.array_equal(out[1][0], out[2][0])
+    # one step per launch: 200 reversed steps plus the recompute and folds
+    assert out[1][1] >= 200 + 180
+    assert out[2][1] < 0.6 * out[1][1], (out[1][1], out[2][1])
+
+
 def test_windowed_shots_equal_cropped_standalone_runs():
     from taichirtm_b200.plan import Plan, ShotGeometry
     rng = np.random.default_rng(9)
