@@ -277,6 +277,10 @@ __global__ void __launch_bounds__(256) adjoint2_kernel(const AdjParams p) {
     zero_row(r2p);
     AdjMat<VEC> m_prev;    // material of row k-1 (the second step's row this iteration)
     float s1[NGRAD][VEC];  // row k-2: partial sums after the first step's contribution
+#pragma unroll
+    for (int gi = 0; gi < NGRAD; ++gi)
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) s1[gi][q] = 0.f;
     AdjIn<VEC> in_nxt;
     AdjMat<VEC> m_nxt;
     load_fwd(F1, ia - 2, in_nxt, false);
@@ -354,10 +358,13 @@ __global__ void __launch_bounds__(256) adjoint2_kernel(const AdjParams p) {
             r2p = r2c;
         }
         // shift: row k-1 becomes row k-2 for the second step's partial sums
+        // (read next iteration exactly when own1 holds now)
+        if (own1) {
 #pragma unroll
-        for (int gi = 0; gi < NGRAD; ++gi)
+            for (int gi = 0; gi < NGRAD; ++gi)
 #pragma unroll
-            for (int q = 0; q < VEC; ++q) s1[gi][q] = gp[gi][q];
+                for (int q = 0; q < VEC; ++q) s1[gi][q] = gp[gi][q];
+        }
         r1p = r1c;
         m_prev = mt;
     }
