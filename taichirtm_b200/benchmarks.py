@@ -12,6 +12,7 @@ c5  Large batched, checkpointed P-SV RTM plus gradient: 4001 x 1601, dt =
 """
 import json
 import math
+import os
 import time
 
 import numpy as np
@@ -27,7 +28,7 @@ def _ev():
     return torch.cuda.Event(enable_timing=True)
 
 
-_ROOT = __import__("os").path.dirname(__import__("os").path.dirname(__import__("os").path.abspath(__file__)))
+_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PEAK_FALLBACK_GBS = 6650.0
 STATE_BYTES_PER_CELL = 40     # P-SV state read + written once per time step, per shot cell
 MATERIAL_BYTES_PER_CELL = 20  # P-SV material read once per time step, per model cell under any window
@@ -36,7 +37,7 @@ KAHAN_IMG_BYTES_PER_CELL = 32  # imaging step: Kahan sum/compensation RMW of u a
 
 def _peak_hbm():
     try:
-        with open(__import__("os").path.join(_ROOT, "MEASURED_PEAKS.json")) as f:
+        with open(os.path.join(_ROOT, "MEASURED_PEAKS.json")) as f:
             return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
         return PEAK_FALLBACK_GBS, "fallback"
@@ -282,7 +283,7 @@ def run_c5(args):
 
 
 def run(args):
-    torch.cuda.set_device(int(__import__("os").environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     if args.workload == "c4":
         return run_c4(args)
     return run_c5(args)
