@@ -220,18 +220,28 @@ int rtm_backward_checkpointed(rtm_plan *plan, const float *wavelets, const float
  * wavelets (3, nsrc, nt), seis (3, nrec, nt), all device pointers; src_ij /
  * rec_ij and *flag (status 0 / 1..3) are host memory.  Every intermediate
  * lives in one static device array of rtm_noalloc_scratch_bytes() bytes
- * (64 MiB, held by every GPU that loads the library until the process exits);
- * a problem needing more (rtm_noalloc_required_bytes) is rejected with
- * RTM_E_RANGE and a message.  The first call on a device looks up that array's
- * device address; make that first call before any stream capture.  All calls
- * share the array: calls that overlap on the GPU (other streams, other host
- * threads) race and must not be issued.  The call synchronises the stream.
- * Results equal rtm_forward's on a one-shot full-grid plan (launch shape vec 2,
- * 16 rows, 4 warps).  Errors: rtm_noalloc_last_error(). */
+ * (64 MiB); a problem needing more (rtm_noalloc_required_bytes) is rejected
+ * with RTM_E_RANGE and a message.
+ *   Set-up: the array belongs to this library's device code, which the CUDA
+ * driver loads on a device the first time it is used there (lazy module
+ * loading): that load reserves the 64 MiB on that device until the process
+ * exits.  rtm_noalloc_prepare() does it for the current device (it looks up
+ * the array's device address and loads every kernel the call launches); call
+ * it once per device in the host's set-up phase, before any stream capture.
+ * A call on a device that was not prepared does the same set-up first, so
+ * that first call is the one that reserves memory.  Later calls allocate
+ * nothing.  After a device reset, prepare again.
+ *   All calls share the array and each clears what must start at zero: calls
+ * that overlap on the GPU (other streams, other host threads) race and must
+ * not be issued.  The call synchronises the stream.  Results equal
+ * rtm_forward's bit for bit on a one-shot full-grid plan (same step kernel
+ * and tables; launch shape vec 2, 16 rows, 4 warps).
+ * Errors: rtm_noalloc_last_error(). */
 int rtm_forward_noalloc(const rtm_grid *grid, int nsrc, const int32_t *src_ij, int nrec,
                         const int32_t *rec_ij, const float *mu, const float *lam, const float *rho,
                         const float *wavelets, float *seis, int check_interval, int32_t *flag,
                         rtm_stream_t stream);
+int rtm_noalloc_prepare(void);
 size_t rtm_noalloc_scratch_bytes(void);
 size_t rtm_noalloc_required_bytes(const rtm_grid *grid, int nsrc, int nrec);
 const char *rtm_noalloc_last_error(void);

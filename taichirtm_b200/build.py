@@ -13,7 +13,7 @@ LIB = os.path.join(LIBDIR, "librtm_b200.so")
 # bounds-checking build (every kernel access checked against the call's buffers)
 DEBUG_LIB = os.path.join(LIBDIR, "librtm_b200_debug.so")
 SOURCES = ["rtm_api.cu", "noalloc.cu"]
-DEPS = ["step_kernels.cuh", "step2_kernels.cuh", "checkpoint_kernels.cuh", "debug_bounds.cuh", "aux_kernels.cuh", "adjoint_kernels.cuh", "adjoint2_kernels.cuh", "noalloc.cu"]
+DEPS = ["plan_host.h", "ckpt_pack.cuh", "step_kernels.cuh", "step2_kernels.cuh", "checkpoint_kernels.cuh", "debug_bounds.cuh", "aux_kernels.cuh", "adjoint_kernels.cuh", "adjoint2_kernels.cuh", "noalloc.cu"]
 # -fmad=false: no FMA contraction, so every cell's FP32 arithmetic follows the
 # reference's expression order exactly and results do not depend on the launch
 # shape the autotuner picks (the kernels are HBM-bound; FLOPs are free).

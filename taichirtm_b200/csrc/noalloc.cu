@@ -9,11 +9,20 @@
 // outputs; every intermediate -- the ping-pong wavefield, the derived material,
 // the source/receiver row tables, the time-major seismogram staging -- lives
 // in one file-scope __device__ array of fixed size (RTM_NOALLOC_SCRATCH_BYTES,
-// 64 MiB).  Every GPU that loads this library holds that array until the
-// process exits.
+// 64 MiB).  Every GPU that loads this library's device code holds that array
+// until the process exits.
+//
+// When the array is reserved.  With lazy module loading (the CUDA default
+// since 12.2) the device code -- the array included -- is loaded on a
+// device the first time host code touches it there.  rtm_noalloc_prepare()
+// does that on the current device: it looks up the array's device address
+// and loads every kernel rtm_forward_noalloc launches, so that a caller can
+// take the reservation in its set-up phase.  A call of rtm_forward_noalloc
+// on a device that was not prepared does the same set-up first.
 //
 // It runs the same fused step kernel as rtm_forward (one launch per time
-// step), so its results equal rtm_forward's for the same inputs.
+// step, launch shape vec 2, 16 rows, 4 warps), and the same host-side table
+// construction (plan_host.h), so its results equal rtm_forward's bit for bit.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,12 +31,12 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/rtm_b200.h"
 #include "aux_kernels.cuh"
+#include "plan_host.h"
 #include "step_kernels.cuh"
 
 using namespace rtm;
@@ -60,26 +69,19 @@ int na_fail(int code, const char *fmt, ...) {
             return na_fail(RTM_E_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));       \
     } while (0)
 
-// Device address of the scratch, looked up once per device with that device
-// current (the first call on each device does it; later calls reuse it).
-constexpr int kMaxDevices = 64;
-void *g_scratch_ptr[kMaxDevices] = {};
-std::mutex g_scratch_mu;
-
+// Device address of the scratch on the current device.  cudaGetSymbolAddress
+// is a host-side table lookup once the module is loaded, so it is done on
+// every call rather than cached: a device reset between calls reloads the
+// module at a new address, and a cached pointer would be stale.
 int scratch_address(void **out) {
     int dev = -1;
     NA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return na_fail(RTM_E_ARG, "device index %d out of range", dev);
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return na_fail(RTM_E_CUDA, "cudaGetSymbolAddress(scratch) failed on device %d: %s", dev,
-                           cudaGetErrorString(e));
-        g_scratch_ptr[dev] = p;
-    }
-    *out = g_scratch_ptr[dev];
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return na_fail(RTM_E_CUDA, "cudaGetSymbolAddress(scratch) failed on device %d: %s", dev,
+                       cudaGetErrorString(e));
+    *out = p;
     return RTM_OK;
 }
 
@@ -109,8 +111,6 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr int kPitchVec = 2;  // launch shape: vec 2, 16 rows per task, 4 warps
 constexpr int kRows = 16;
 
-int pitch_of(int nz) { return ((((nz + 119) / 120) * 120 + 8 + COL_OFF) + 31) / 32 * 32; }
-
 Layout layout_for(const rtm_grid &g, int nsrc, int nrec, int n_work) {
     Layout L{};
     size_t off = 0;
@@ -119,7 +119,7 @@ Layout layout_for(const rtm_grid &g, int nsrc, int nrec, int n_work) {
         off += align256(bytes);
         return o;
     };
-    const int P = pitch_of(g.nz);
+    const int P = layout_pitch(g.nz);
     const size_t grid_f = (size_t)(g.nx + 2) * P * sizeof(float);
     for (int b = 0; b < 2; ++b)
         for (int f = 0; f < NFIELD; ++f) {
@@ -149,13 +149,15 @@ int n_work_for(const rtm_grid &g) {
     return ((g.nx + kRows - 1) / kRows) * strips;
 }
 
+// The checks of rtm_plan_create for one shot on the whole grid: the grid,
+// then the shot (absorbing_frame no wider than its rows, positions inside).
 int validate(const rtm_grid *g, int nsrc, const int32_t *src_ij, int nrec, const int32_t *rec_ij) {
     if (!g) return na_fail(RTM_E_ARG, "null grid");
-    if (g->nx < 3 || g->nz < 3 || g->nt <= 0) return na_fail(RTM_E_ARG, "grid must be >= 3x3 with nt > 0");
-    if (!(g->fs > 0) || !(g->dx > 0) || !(g->dz > 0)) return na_fail(RTM_E_ARG, "fs, dx, dz must be positive");
-    if (g->modes < 1 || g->modes > 3) return na_fail(RTM_E_ARG, "modes must be RTM_PSV, RTM_SH or RTM_BOTH");
-    if (g->absorbing_frame < 0 || g->absorbing_frame > g->nx || g->absorbing_frame > g->nz)
-        return na_fail(RTM_E_ARG, "absorbing_frame %d outside [0, min(nx, nz)]", g->absorbing_frame);
+    if (const char *bad = check_grid(*g))
+        return na_fail(RTM_E_ARG, "%s (nx=%d nz=%d nt=%d absorbing_frame=%d)", bad, g->nx, g->nz, g->nt,
+                       g->absorbing_frame);
+    if (g->absorbing_frame > g->nx)
+        return na_fail(RTM_E_ARG, "absorbing_frame %d wider than the %d rows of the grid", g->absorbing_frame, g->nx);
     if (nsrc < 0 || nrec < 0 || (nsrc && !src_ij) || (nrec && !rec_ij))
         return na_fail(RTM_E_ARG, "bad source/receiver arrays");
     for (int k = 0; k < nsrc; ++k)
@@ -165,6 +167,28 @@ int validate(const rtm_grid *g, int nsrc, const int32_t *src_ij, int nrec, const
         if (rec_ij[2 * k] < 0 || rec_ij[2 * k] >= g->nx || rec_ij[2 * k + 1] < 0 || rec_ij[2 * k + 1] >= g->nz)
             return na_fail(RTM_E_ARG, "receiver %d at (%d, %d) outside the grid", k, rec_ij[2 * k], rec_ij[2 * k + 1]);
     return RTM_OK;
+}
+
+// Loads every kernel rtm_forward_noalloc launches on the current device
+// (cudaFuncGetAttributes makes the driver load a lazily loaded function), so
+// that no module load -- which reserves device memory -- happens later.
+int load_kernels() {
+    cudaFuncAttributes a;
+    NA_TRY(cudaFuncGetAttributes(&a, step_kernel<0, RTM_PSV, 2>));
+    NA_TRY(cudaFuncGetAttributes(&a, step_kernel<0, RTM_SH, 2>));
+    NA_TRY(cudaFuncGetAttributes(&a, step_kernel<0, RTM_BOTH, 2>));
+    NA_TRY(cudaFuncGetAttributes(&a, setup_material_kernel));
+    NA_TRY(cudaFuncGetAttributes(&a, transpose_kernel));
+    return RTM_OK;
+}
+
+// The set-up: the scratch's device address on the current device and every
+// kernel loaded.  Both are host-side lookups once the module is loaded, so
+// every call repeats them instead of caching: a device reset between calls
+// reloads the module (at a new address), and this finds it again.
+int prepare_current_device(void **scratch) {
+    if (int rc = scratch_address(scratch)) return rc;
+    return load_kernels();
 }
 
 }  // namespace
@@ -179,6 +203,11 @@ size_t rtm_noalloc_required_bytes(const rtm_grid *grid, int nsrc, int nrec) {
 }
 
 const char *rtm_noalloc_last_error(void) { return g_na_err.c_str(); }
+
+int rtm_noalloc_prepare(void) {
+    void *p = nullptr;
+    return prepare_current_device(&p);
+}
 
 int rtm_forward_noalloc(const rtm_grid *grid, int nsrc, const int32_t *src_ij, int nrec,
                         const int32_t *rec_ij, const float *mu, const float *lam, const float *rho,
@@ -196,25 +225,16 @@ int rtm_forward_noalloc(const rtm_grid *grid, int nsrc, const int32_t *src_ij, i
                        "rtm_forward_noalloc (nx=%d nz=%d nt=%d nrec=%d); use rtm_forward",
                        L.total, (unsigned long long)RTM_NOALLOC_SCRATCH_BYTES, g.nx, g.nz, g.nt, nrec);
     void *base_v = nullptr;
-    if (int rc = scratch_address(&base_v)) return rc;
+    if (int rc = prepare_current_device(&base_v)) return rc;  // loads the module on a device's first call
     unsigned char *base = static_cast<unsigned char *>(base_v);
     cudaStream_t s = (cudaStream_t)stream;
-    const int P = pitch_of(g.nz);
+    const int P = layout_pitch(g.nz);
 
-    // host-side tables (same construction as rtm_plan_create for one full-grid shot)
+    // host-side tables: the construction of rtm_plan_create (plan_host.h)
     std::vector<int> src_ptr, rec_ptr;
     std::vector<int2> src_ent, rec_ent;
-    auto rows = [&](int n, const int32_t *ij, std::vector<int> &ptr, std::vector<int2> &ent) {
-        std::vector<std::vector<int2>> byrow(g.nx);
-        for (int k = 0; k < n; ++k) byrow[ij[2 * k]].push_back(make_int2(ij[2 * k + 1], k));
-        for (int i = 0; i < g.nx; ++i) {
-            ptr.push_back((int)ent.size());
-            for (auto &e : byrow[i]) ent.push_back(e);
-        }
-        ptr.push_back((int)ent.size());
-    };
-    rows(nsrc, src_ij, src_ptr, src_ent);
-    rows(nrec, rec_ij, rec_ptr, rec_ent);
+    append_row_table(g.nx, g.nz, nsrc, src_ij, 0, src_ptr, src_ent);  // positions checked by validate()
+    append_row_table(g.nx, g.nz, nrec, rec_ij, 0, rec_ptr, rec_ent);
     std::vector<int4> work;
     const int strips = (g.nz + 30 * kPitchVec - 1) / (30 * kPitchVec);
     for (int ia = 0; ia < g.nx; ia += kRows)
@@ -226,11 +246,7 @@ int rtm_forward_noalloc(const rtm_grid *grid, int nsrc, const int32_t *src_ij, i
     shot.row_off = 0;
     shot.src_row0 = 0;
     shot.rec_row0 = 0;
-    std::vector<float> prof(g.absorbing_frame > 0 ? g.absorbing_frame : 1, 1.0f);
-    for (int d = 0; d < g.absorbing_frame; ++d) {
-        const double diff = (double)(g.absorbing_frame - d);
-        prof[d] = (float)std::exp((-(0.0053 * 0.0053) * diff) * diff);
-    }
+    const std::vector<float> prof = sponge_profile(g.absorbing_frame);
     // The tables live in pageable host memory that goes out of scope when this
     // call returns, so these copies complete before it does.
     NA_TRY(cudaMemcpyAsync(base + L.sponge, prof.data(), prof.size() * sizeof(float), cudaMemcpyHostToDevice, s));

@@ -18,6 +18,7 @@
 #include "aux_kernels.cuh"
 #include "step2_kernels.cuh"
 #include "adjoint2_kernels.cuh"
+#include "plan_host.h"
 #include "step_kernels.cuh"
 
 using namespace rtm;
@@ -53,8 +54,6 @@ int dalloc(T **p, size_t n) {
     CUDA_TRY(cudaMalloc((void **)p, n * sizeof(T)));
     return 0;
 }
-
-int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
 // NVTX range around an entry point: the phases show up by name in Nsight
 // Systems; without a profiler attached it costs a call that returns.
@@ -452,12 +451,8 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
     if (!grid || !shots || !out || nshots <= 0) return fail(RTM_E_ARG, "null argument or nshots <= 0");
     *out = nullptr;
     const rtm_grid g = *grid;
-    if (g.nx < 3 || g.nz < 3) return fail(RTM_E_ARG, "grid must be at least 3x3 (nx=%d nz=%d)", g.nx, g.nz);
-    if (g.nt <= 0) return fail(RTM_E_ARG, "nt must be positive");
-    if (!(g.fs > 0) || !(g.dx > 0) || !(g.dz > 0)) return fail(RTM_E_ARG, "fs, dx, dz must be positive");
-    if (g.modes < 1 || g.modes > 3) return fail(RTM_E_ARG, "modes must be RTM_PSV, RTM_SH or RTM_BOTH");
-    if (g.absorbing_frame < 0 || g.absorbing_frame > g.nz)
-        return fail(RTM_E_ARG, "absorbing_frame %d outside [0, nz]", g.absorbing_frame);
+    if (const char *bad = check_grid(g))
+        return fail(RTM_E_ARG, "%s (nx=%d nz=%d nt=%d absorbing_frame=%d)", bad, g.nx, g.nz, g.nt, g.absorbing_frame);
     rtm_plan *p = new rtm_plan();
     p->g = g;
     p->nshots = nshots;
@@ -477,10 +472,7 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
     }
     const int W = 30 * p->vec;
     p->nstrips = (g.nz + W - 1) / W;
-    // Lanes touch columns [-vec, nstrips*W + vec); with 4 padding columns on
-    // the left this fits in ceil(nz/120)*120 + 8 for every vec, so the pitch
-    // (and every caller-visible layout) does not depend on the launch shape.
-    p->pitch = round_up(((g.nz + 119) / 120) * 120 + 8 + COL_OFF, 32);
+    p->pitch = layout_pitch(g.nz);
 
     // shots, row tables, work list
     std::vector<int> src_ptr, rec_ptr;
@@ -511,18 +503,10 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
         // per-row CSR, stable in the given order (duplicates accumulate in order)
         auto build = [&](int n, const int32_t *ij, int base, std::vector<int> &ptr,
                          std::vector<int2> &ent, const char *what) -> int {
-            std::vector<std::vector<int2>> byrow(sh.nx);
-            for (int k = 0; k < n; ++k) {
-                const int i = ij[2 * k], j = ij[2 * k + 1];
-                if (i < 0 || i >= sh.nx || j < 0 || j >= g.nz)
-                    return fail(RTM_E_ARG, "shot %d: %s %d at (%d, %d) outside the %dx%d window", s, what, k, i, j, sh.nx, g.nz);
-                byrow[i].push_back(make_int2(j, base + k));
-            }
-            for (int i = 0; i < sh.nx; ++i) {
-                ptr.push_back((int)ent.size());
-                for (auto &e : byrow[i]) ent.push_back(e);
-            }
-            ptr.push_back((int)ent.size());
+            const int k = append_row_table(sh.nx, g.nz, n, ij, base, ptr, ent);
+            if (k >= 0)
+                return fail(RTM_E_ARG, "shot %d: %s %d at (%d, %d) outside the %dx%d window", s, what, k, ij[2 * k],
+                            ij[2 * k + 1], sh.nx, g.nz);
             return 0;
         };
         if (build(sh.nsrc, sh.src_ij, p->nsrc_total, src_ptr, src_ent, "source") ||
@@ -601,13 +585,7 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
         delete p;
         return rc < 0 ? rc : RTM_E_NOMEM;
     }
-    // sponge profile g(d) = exp(-(a (FW - d))^2), a = 0.0053 (forward_modeling.py:218-240)
-    std::vector<float> prof(std::max(g.absorbing_frame, 1), 1.0f);
-    const double a = 0.0053;
-    for (int d = 0; d < g.absorbing_frame; ++d) {
-        const double diff = (double)(g.absorbing_frame - d);
-        prof[d] = (float)std::exp((-(a * a) * diff) * diff);
-    }
+    const std::vector<float> prof = sponge_profile(g.absorbing_frame);
     auto H2D = [](void *dst, const void *src, size_t bytes) {
         return bytes ? cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) : cudaSuccess;
     };

@@ -29,18 +29,30 @@ def shard_shots(costs: Sequence[float], world_size: int, rank: int) -> List[int]
     return [i for i in range(len(costs)) if owner[i] == rank]
 
 
+def collective_device(group=None) -> torch.device:
+    """The device the process group's collectives run on: this rank's current
+    CUDA device under NCCL, the host under gloo.  Every collective of this
+    module puts its tensors there, on the success and the failure path alike,
+    so a failing rank never issues a collective that the others cannot
+    match."""
+    if dist.get_backend(group) == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
+
+
 def reduce_result(local: torch.Tensor, status: int, group=None) -> torch.Tensor:
     """Sum ``local`` (an FP64 image/gradient stack) over ranks after agreeing
     that every rank succeeded.  Raises RuntimeError on every rank if any
-    rank reported a non-zero status."""
-    dev = local.device
-    st = torch.tensor([int(status)], dtype=torch.int64, device=dev)
+    rank reported a non-zero status.  The status tensor lives on the group's
+    collective device (``collective_device``), whatever ``local`` is, so a
+    rank that failed before it had a result takes the same first step."""
+    st = torch.tensor([int(status)], dtype=torch.int64, device=collective_device(group))
     dist.all_reduce(st, op=dist.ReduceOp.MAX, group=group)
     if int(st.item()) != 0:
         raise RuntimeError(f"a rank reported propagation status {int(st.item())}; result discarded")
-    out = local.clone()
+    out = local.to(collective_device(group), torch.float64).clone()
     dist.all_reduce(out, op=dist.ReduceOp.SUM, group=group)
-    return out
+    return out.to(local.device)
 
 
 def run_sharded(costs: Sequence[float], compute: Callable[[List[int]], torch.Tensor], group=None) -> torch.Tensor:
@@ -60,8 +72,9 @@ def run_sharded(costs: Sequence[float], compute: Callable[[List[int]], torch.Ten
         local = None
         status = 99
     if local is None:
-        # same collective steps as the success path
-        local = torch.zeros(1, dtype=torch.float64)
+        # same collective steps as the success path: the status all-reduce on
+        # the group's device (reduce_result), after which every rank raises
+        local = torch.zeros(1, dtype=torch.float64, device=collective_device(group))
     try:
         return reduce_result(local, status, group)
     except RuntimeError:

@@ -25,16 +25,15 @@ def load_rtm_results(directory: str, pattern: str = "*.npz") -> List[Dict[str, A
 
 
 def _sum_fp64(arrays):
-    if torch.cuda.is_available():
-        acc = None
-        for a in arrays:
-            t = torch.as_tensor(np.asarray(a)).to("cuda", torch.float64)
-            acc = t if acc is None else acc + t
-        return acc.cpu().numpy()
-    acc = np.zeros_like(np.asarray(arrays[0]), dtype=np.float64)
+    """FP64 sum of the per-shot images on the GPU.  There is no host path:
+    without a visible CUDA device this raises."""
+    from .plan import require_cuda
+    require_cuda()
+    acc = None
     for a in arrays:
-        acc += a
-    return acc
+        t = torch.as_tensor(np.asarray(a)).to("cuda", torch.float64)
+        acc = t if acc is None else acc + t
+    return acc.cpu().numpy()
 
 
 def stack_rtm_images(results: List[Dict[str, Any]], subtract_mean: bool = True) -> Dict[str, np.ndarray]:

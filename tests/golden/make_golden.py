@@ -2,10 +2,10 @@
 (``src/forward_modeling.py``, ``src/backward_modeling.py``, ``src/rtm.py``)
 under the NumPy Taichi stub in ``taichi_stub.py`` (FP64, serial, tiny grids).
 
-Test infrastructure only.  Run in a container that has the reference checked
-out (default ``/root/reference``; override with ``TAICHIRTM_REF``):
+Test infrastructure only.  Run where the reference is checked out, naming its
+root in ``TAICHIRTM_REF`` (the directory that holds ``src/``):
 
-    python tests/golden/make_golden.py
+    TAICHIRTM_REF=<path to TaichiRTM> python tests/golden/make_golden.py
 
 Writes ``tests/golden/*.npz``.  The fixtures are committed; the GPU box never
 needs the reference.
@@ -18,10 +18,12 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("TAICHIRTM_REF", "/root/reference")
+REF = os.environ.get("TAICHIRTM_REF", "")
 
 
 def load_reference():
+    if not REF or not os.path.isdir(os.path.join(REF, "src")):
+        raise SystemExit("set TAICHIRTM_REF to the TaichiRTM checkout (the directory holding src/)")
     os.environ.setdefault("TQDM_DISABLE", "1")
     sys.path.insert(0, HERE)
     import taichi_stub  # noqa: E402

@@ -78,3 +78,41 @@ def test_run_sharded_gloo(tmp_path, fail_rank):
         # through the status exchange and raises instead of hanging
         assert res[fail_rank] == "FloatingPointError"
         assert res[1 - fail_rank] == "RuntimeError"
+
+
+def _record_collectives(monkeypatch, backend, fail):
+    """run_sharded on a stand-in two-rank group whose all-reduce records
+    (device, dtype, shape) and returns the local values."""
+    from taichirtm_b200 import distributed as D
+    calls = []
+    monkeypatch.setattr(D.dist, "get_world_size", lambda group=None: 2)
+    monkeypatch.setattr(D.dist, "get_rank", lambda group=None: 0)
+    monkeypatch.setattr(D.dist, "get_backend", lambda group=None: backend)
+    monkeypatch.setattr(D.dist, "all_reduce",
+                        lambda t, op=None, group=None: calls.append((t.device.type, t.dtype, tuple(t.shape))))
+
+    def compute(idx):
+        if fail:
+            raise FloatingPointError("code 3")
+        return torch.ones((3, 4, 5), dtype=torch.float64)
+    try:
+        D.run_sharded([1, 2, 3], compute)
+    except FloatingPointError:
+        pass
+    return calls
+
+
+def test_success_and_failure_paths_issue_the_same_status_collective(monkeypatch):
+    ok = _record_collectives(monkeypatch, "gloo", fail=False)
+    bad = _record_collectives(monkeypatch, "gloo", fail=True)
+    assert ok[0] == bad[0] == ("cpu", torch.int64, (1,))  # the status all-reduce, identical on both paths
+    assert ok[1] == ("cpu", torch.float64, (3, 4, 5)) and len(bad) == 1  # data only after a clean status
+
+
+def test_collective_device_follows_the_backend(monkeypatch):
+    from taichirtm_b200 import distributed as D
+    monkeypatch.setattr(D.dist, "get_backend", lambda group=None: "nccl")
+    monkeypatch.setattr(D.torch.cuda, "current_device", lambda: 3)
+    assert D.collective_device() == torch.device("cuda", 3)
+    monkeypatch.setattr(D.dist, "get_backend", lambda group=None: "gloo")
+    assert D.collective_device() == torch.device("cpu")

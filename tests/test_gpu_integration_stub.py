@@ -1,31 +1,17 @@
-"""The ctypes stub that INTEGRATION.md gives a TaichiRTM maintainer, executed as
-written (only the library path is made absolute), against the package's own
-ForwardModeling: the same seismograms and status code."""
-import os
-import re
-
+"""The ctypes binding a TaichiRTM maintainer would add
+(taichirtm_b200/reference_binding.py), loaded on the in-tree library and run
+against the package's own ForwardModeling: the same seismograms and status
+code."""
 import numpy as np
 import pytest
 import torch
 
 pytestmark = pytest.mark.gpu
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-
-
-def _stub_namespace():
-    from taichirtm_b200 import _lib
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    block = re.search(r"### ctypes stub.*?```python\n(.*?)```", text, re.S).group(1)
-    lib = _lib.lib()._name  # the in-tree librtm_b200.so the package loads
-    ns = {}
-    exec(compile(block.replace('"librtm_b200.so"', repr(lib)), "INTEGRATION.md", "exec"), ns)
-    return ns
-
 
 def test_integration_stub_matches_forward_modeling():
-    from taichirtm_b200 import ForwardModeling
-    ns = _stub_namespace()
+    from taichirtm_b200 import ForwardModeling, _lib, reference_binding
+    lib = reference_binding.load(_lib.lib()._name)  # the in-tree librtm_b200.so the package loads
     nx, nz, nt, fw = 60, 48, 120, 10
     rng = np.random.default_rng(2)
     vp = 2200.0 + 300.0 * rng.random((nx, nz))
@@ -42,7 +28,7 @@ def test_integration_stub_matches_forward_modeling():
     dev = torch.device("cuda")
     d = {k: torch.as_tensor(v, device=dev).contiguous() for k, v in dict(mu=mu, lam=lam, rho=rho, wav=wav).items()}
     seis = torch.zeros((3, len(rec), nt), dtype=torch.float32, device=dev)
-    flag = ns["run_forward"](nx, nz, 5.0, 5.0, nt, 2000.0, fw, d["mu"], d["lam"], d["rho"], src, rec, d["wav"], seis,
+    flag = reference_binding.run_forward(lib, nx, nz, 5.0, 5.0, nt, 2000.0, fw, d["mu"], d["lam"], d["rho"], src, rec, d["wav"], seis,
                              stream=torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     fo = ForwardModeling(nx=nx, nz=nz, dx=5.0, dz=5.0, nt=nt, fs=2000.0, absorbing_frame=fw, mu_field=mu,

@@ -80,8 +80,7 @@ def test_legacy_kwargs_constructor_warns():
     assert r.nt == 5 and r.absorbing_frame == 50 and r.isnap == 216
 
 
-def test_imaging_stack_and_npz_roundtrip(tmp_path):
-    from taichirtm_b200 import imaging
+def _imaging_results(tmp_path):
     rng = np.random.default_rng(1)
     res = []
     for k in range(3):
@@ -89,8 +88,35 @@ def test_imaging_stack_and_npz_roundtrip(tmp_path):
                  w=rng.standard_normal((6, 4)).astype(np.float32), offset=2.0, dx=0.5, dz=0.5, nx=6, nz=4)
         np.savez_compressed(tmp_path / f"s{k}.npz", **d)
         res.append(d)
+    return res
+
+
+def test_imaging_npz_load_and_save(tmp_path):
+    from taichirtm_b200 import imaging
+    res = _imaging_results(tmp_path)
     loaded = imaging.load_rtm_results(str(tmp_path))
     assert len(loaded) == 3 and all("filepath" in x for x in loaded)
+    st = dict(u=res[0]["u"].T, v=res[0]["v"].T, w=res[0]["w"].T, xmin=-2.0, xmax=1.0, zmin=0.0, zmax=2.0)
+    imaging.save_stacked_results(st, str(tmp_path / "out" / "stack.npz"))
+    assert set(np.load(tmp_path / "out" / "stack.npz").files) == {"u", "v", "w", "xmin", "xmax", "zmin", "zmax"}
+
+
+def test_imaging_stack_needs_a_gpu(tmp_path):
+    """The cross-shot sum runs on the GPU in FP64; with no GPU visible it
+    raises instead of summing on the host."""
+    import torch
+
+    from taichirtm_b200 import imaging
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    with pytest.raises(RuntimeError, match="CUDA"):
+        imaging.stack_rtm_images(_imaging_results(tmp_path))
+
+
+@pytest.mark.gpu
+def test_imaging_stack_and_npz_roundtrip(tmp_path):
+    from taichirtm_b200 import imaging
+    res = _imaging_results(tmp_path)
     st = imaging.stack_rtm_images(res, subtract_mean=True)
     ref = sum(x["u"].astype(np.float64) for x in res).T
     ref = ref - ref.mean()
