@@ -12,15 +12,20 @@ Observed data are modelled on the true model before timing.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Under torchrun every rank migrates its own 64-shot batch (weak scaling) and
-the stacked images are summed across ranks with one FP64 all-reduce.
+Under torchrun the job is N copies of the 64-shot survey (weak scaling: 64
+shots per GPU); taichirtm_b200.distributed.shard_shots splits them across the
+ranks by cost and reduce_result sums the stacked images with one FP64
+all-reduce after a status agreement, the shipped sharded path.
+
+Besides the headline line, the default run also times, with their own clock
+records, the FWI gradient (8 shots on 1201 x 401, batched against one shot per
+problem) and checkpointed RTM (the same 64 shots with sqrt(nt) checkpoints,
+batched against one shot per plan): keys "gradient" and "checkpointed_rtm".
 """
 import argparse
 import json
 import os
-import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -40,6 +45,15 @@ PEAK_FALLBACK_GBS = 6650.0
 def workload_desc(nshots, nt):
     return (f"batched P-SV RTM: {nshots} shots on a 2001x801 model (dx=5 m, dt=0.5 ms, nt={nt}), "
             "windows of U{200..800} receivers +- 50-cell sponge, isnap=16, Kahan imaging, FP64 stack")
+
+
+def bench_config(nshots, nt, world, cells):
+    """The workload as both arms name it (the same dict in both lines)."""
+    return dict(workload=workload_desc(nshots, nt), shots_per_gpu=nshots, cells_per_shot_step=int(cells),
+                grid="2001x801", nt=nt, isnap=ISNAP,
+                l2="no flush: per-step working set (state 2.6 GB + snapshots 48 GB) >> 126 MB L2",
+                parallelism=f"{world} x {nshots} shots sharded by cost across {world} GPU(s), "
+                            "FP64 all-reduce of the image")
 
 
 def peak_hbm():
@@ -62,110 +76,79 @@ def ncu_traffic_per_cell(tsteps=1):
         return None
 
 
-class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
-
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-
-    def __init__(self):
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        self.p = None
-
-    def start(self):
-        try:
-            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS,
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
-                                      stdout=self.f, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.p = None
-
-    def stop(self, gpu_index=None):
-        if self.p is None:
-            return None
-        self.p.terminate()
-        try:
-            self.p.wait(timeout=5)
-        except Exception:
-            self.p.kill()
-        self.f.seek(0)
-        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
-        os.unlink(self.f.name)
-        if gpu_index is not None:
-            sel = [r for r in rows if r[0].strip() == str(gpu_index)]
-            rows = sel or rows
-        if not rows:
-            return None
-        sm = np.array([float(r[1]) for r in rows])
-        mx = max(float(r[2]) for r in rows)
-        pw = np.array([float(r[3]) if r[3].strip() not in ("[N/A]", "N/A") else 0 for r in rows])
-        load = sm[pw > 0.5 * pw.max()] if pw.max() > 0 else sm
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
-        return dict(sm_mhz=float(np.median(load)), sm_max_mhz=mx, reasons=reasons, samples=len(rows))
-
-
 def build_workload(nt):
     from taichirtm_b200 import synthetic as S
     return S.config3(nt=nt)
 
 
 # --------------------------------------------------------------------------- CPU
-def cpu_rtm_sample(survey, target_s=12.0, modes=3):
+def cpu_rtm_shot(survey, k, n_run=None, modes=3):
     """The reference algorithm on the host cores (C/OpenMP FP32 restatement of
     src/forward_modeling.py + src/backward_modeling.py, both P-SV and SH as the
-    reference always advances): one shot of the workload, the time loop
-    truncated to a bounded number of steps per phase, scaled to one shot."""
+    reference always advances): shot k of the workload on its window, forward
+    with snapshots every ISNAP steps, backward with imaging.  n_run None = the
+    whole time axis.  Returns (seconds, dict describing the run)."""
     from oracle import c_oracle
-    sh = survey.shots[0]
+    sh = survey.shots[k]
     mu, lam, rho = survey.material(migration=True)
     mu, lam, rho = (np.ascontiguousarray(x[sh.x0:sh.x0 + sh.nx]) for x in (mu, lam, rho))
     nthreads = os.cpu_count() or 1
     nt = survey.nt
+    n_run = nt if n_run is None else int(min(nt, n_run))
     kw = dict(dx=survey.dx, dz=survey.dz, nt=nt, fs=survey.fs, fw=survey.fw, dtype=np.float32,
               modes=modes, nthreads=nthreads)
-    probe = 20
-    t0 = time.perf_counter()
-    c_oracle.forward(mu, lam, rho, src=sh.src, wu=sh.wavelets[0], wv=sh.wavelets[1], ww=sh.wavelets[2],
-                     rec=sh.rec, nt_run=probe, **kw)
-    per_step = (time.perf_counter() - t0) / probe
-    n_run = int(max(20, min(nt, target_s / 2.0 / max(per_step, 1e-6))))
     t0 = time.perf_counter()
     f = c_oracle.forward(mu, lam, rho, src=sh.src, wu=sh.wavelets[0], wv=sh.wavelets[1], ww=sh.wavelets[2],
                          rec=sh.rec, nt_run=n_run, save=True, isnap=ISNAP, **kw)
-    t_f = time.perf_counter() - t0
-    t0 = time.perf_counter()
     c_oracle.backward(mu, lam, rho, rec=sh.rec, obs=np.zeros((3, len(sh.rec), nt), np.float32),
                       snaps=f["snaps"], isnaps=np.arange(1, nt // ISNAP + 1) * ISNAP,
                       num_snaps=nt // ISNAP, isnap=ISNAP, nt_run=n_run, **kw)
-    t_b = time.perf_counter() - t0
-    sec_per_shot = (t_f + t_b) * nt / n_run
-    cells = sh.nx * survey.nz
-    return dict(value=1.0 / sec_per_shot, unit="shots/s", cores=nthreads, kind="port",
-                gcell_upd_per_s=2 * cells * nt / sec_per_shot / 1e9,
-                sample=(f"shot 0 ({sh.nx}x{survey.nz} window), {n_run} of {nt} steps per phase "
+    sec = time.perf_counter() - t0
+    return sec, dict(cores=nthreads, kind="port", cells=sh.nx * survey.nz, nx=sh.nx, n_run=n_run)
+
+
+def cpu_rtm_sample(survey):
+    """cpu_baseline leg of the GPU arm: shot 0 migrated in full on the host
+    cores (a bounded sample of the workload, about 5 s on 16 cores)."""
+    sec, d = cpu_rtm_shot(survey, 0)
+    nt = survey.nt
+    return dict(value=1.0 / sec, unit="shots/s", cores=d["cores"], kind="port",
+                gcell_upd_per_s=2 * d["cells"] * nt / sec / 1e9,
+                sample=(f"shot 0 ({d['nx']}x{survey.nz} window), all {nt} steps of both phases "
                         f"(forward with snapshots + backward with imaging), FP32, P-SV+SH as the "
-                        f"reference runs, scaled x{nt / n_run:.1f} to one shot"))
+                        f"reference runs"))
 
 
 def reference_arm(args, rank):
+    """The reference's algorithm on the host cores (Taichi cannot be installed
+    offline, so the C/OpenMP restatement of its kernels): every step is one
+    whole shot of the workload -- shots taken in turn, all nt steps of the
+    forward with snapshots and the backward with imaging -- so ms_per_step is
+    the measured time of one step and value = timed shots / timed seconds."""
     if rank != 0:
         return 0
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     survey = build_workload(3000)
     import platform
-    vals = []
+    times = []
+    info = None
     for i in range(args.warmup + args.steps):
-        r = cpu_rtm_sample(survey, target_s=4.0)
+        sec, info = cpu_rtm_shot(survey, i % len(survey.shots))
         if i >= args.warmup:
-            vals.append(r["value"])
-    v = float(np.mean(vals))
-    line = dict(impl="reference", metric=METRIC, value=v, unit="shots/s", n_gpus=args.gpus,
-                steps=args.steps, warmup=args.warmup, ms_per_step=1000.0 / v * 1.0,
+            times.append(sec)
+    total = float(sum(times))
+    v = args.steps / total
+    cells = sum(s.nx for s in survey.shots) * survey.nz
+    sample = (f"{args.steps} whole shots (shots {args.warmup % 64}.. in turn, after {args.warmup} untimed), "
+              f"all 3000 steps of both phases each, FP32, P-SV+SH as the reference runs, "
+              f"{info['cores']} host threads")
+    line = dict(impl="reference", metric=METRIC, value=v, unit="shots/s", n_gpus=world,
+                steps=args.steps, warmup=args.warmup, ms_per_step=1000.0 * total / args.steps,
                 higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
-                config=dict(workload=workload_desc(64, 3000) + " (per-shot rate on a bounded sample)",
-                            host=platform.processor() or platform.machine()),
-                cpu_baseline=dict(value=v, unit="shots/s", cores=r["cores"], kind="port", sample=r["sample"]),
+                config=bench_config(64, 3000, world, cells),
+                step="one whole shot of the workload on the host cores",
+                host=platform.processor() or platform.machine(),
+                cpu_baseline=dict(value=v, unit="shots/s", cores=info["cores"], kind="port", sample=sample),
                 e2e=dict(value=v, unit="shots/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0),
                 note="Taichi (the reference's runtime) is not installable offline; the reference arm "
                      "times the C/OpenMP restatement of its kernels on all host cores")
@@ -182,6 +165,7 @@ def plain_single_shot(args, rank):
         return 0
     import torch
     from taichirtm_b200 import autotune, synthetic as S
+    from taichirtm_b200.benchmarks import ClockSampler
     from taichirtm_b200.plan import PSV, SH, Plan, ShotGeometry
     from oracle import c_oracle
     cfg = S.config1() if args.workload == "c1" else S.config2()
@@ -213,12 +197,14 @@ def plain_single_shot(args, rank):
         f1, f2, img = rtm()
     assert int(f1.max()) == 0 and int(f2.max()) == 0
     torch.cuda.synchronize()
+    clk = ClockSampler().start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(args.steps):
         rtm()
     e1.record()
     torch.cuda.synchronize()
+    clocks = clk.stop()
     ms = e0.elapsed_time(e1) / args.steps
     cells = cfg.nx * cfg.nz
     # both modes advanced, as the reference always does (the skipped mode is
@@ -256,8 +242,8 @@ def plain_single_shot(args, rank):
                 warmup=args.warmup, ms_per_step=round(ms, 3), higher_is_better=True, scaling="weak",
                 vs_baseline=None, dtype="f32", data="synthetic",
                 config=dict(workload=cfg.name + f": {cfg.nx}x{cfg.nz}, nt={cfg.nt}, isnap={isnap}, one shot, "
-                            "forward with snapshots + backward with imaging", launch_shape=tune),
-                gcell_upd_per_s=round(2 * cells * cfg.nt / (ms / 1000.0) / 1e9, 2),
+                            "forward with snapshots + backward with imaging"),
+                launch_shape=tune, clocks=clocks, gcell_upd_per_s=round(2 * cells * cfg.nt / (ms / 1000.0) / 1e9, 2),
                 us_per_step=round(ms * 1000.0 / (2 * cfg.nt), 2),
                 both_modes=dict(shots_per_s=round(1000.0 / ms_both, 3),
                                 note="P-SV and SH both advanced, as the reference does"),
@@ -279,6 +265,11 @@ def main():
     ap.add_argument("--shots", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the one-shot-per-launch leg")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the checkpointed-RTM and FWI-gradient legs of the default workload")
+    ap.add_argument("--ckpt-dtype", default=None, choices=["f32", "f16", "bf16", "i16"],
+                    help="checkpoint storage of the checkpointed-RTM leg and of c5 (default i16: 16-bit block "
+                         "floating point, one scale per 60-column block)")
     ap.add_argument("--tune", default=None,
                     help='fixed launch shape as JSON, e.g. \'{"vec": 2, "rows": 32, "warps": 1, "tsteps": 2}\' '
                          "(default: the autotuner's choice)")
@@ -299,8 +290,9 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from taichirtm_b200.batch import BatchedRTM, survey_shots, survey_wavelets
-    from taichirtm_b200.distributed import reduce_result
+    from taichirtm_b200.batch import BatchedRTM, survey_shots
+    from taichirtm_b200.benchmarks import ClockSampler
+    from taichirtm_b200.distributed import reduce_result, shard_shots
     from taichirtm_b200.plan import PSV
 
     torch.cuda.set_device(local)
@@ -311,8 +303,14 @@ def main():
     dev = torch.device("cuda", local)
     survey = build_workload(args.nt or 3000)
     survey.shots = survey.shots[: args.shots]
+    # the job: `world` copies of the survey's shots, split across the ranks by
+    # cost (window cells) -- each rank gets one copy of every shot
+    base = survey.shots
+    job = [k for _ in range(world) for k in range(len(base))]
+    mine = shard_shots([base[k].nx * survey.nz for k in job], world, rank)
+    survey.shots = [base[job[i]] for i in mine]
     shots = survey_shots(survey)
-    wav = torch.as_tensor(survey_wavelets(survey)).to(dev)
+    wav = torch.as_tensor(np.concatenate([s.wavelets for s in survey.shots], axis=1)).to(dev)
     mu_t, lam_t, rho_t = survey.material()
     mu_m, lam_m, rho_m = survey.material(migration=True)
 
@@ -357,8 +355,7 @@ def main():
         reduce_result(torch.zeros(1, dtype=torch.float64, device=dev), status)  # all ranks agree or raise
     elif status:
         raise FloatingPointError(f"propagation became non-finite (code {status})")
-    sampler = ClockSampler()
-    sampler.start()
+    sampler = ClockSampler().start()
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     launches = 0
     t_start = torch.cuda.Event(enable_timing=True)
@@ -377,7 +374,7 @@ def main():
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier(device_ids=[local])
-    clocks = sampler.stop(os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0] or None)
+    clocks = sampler.stop()
     ms = t_start.elapsed_time(t_end)
     fwd_ms = sum(e[0].elapsed_time(e[1]) for e in evs)
     bwd_ms = sum(e[1].elapsed_time(e[2]) for e in evs)
@@ -386,7 +383,10 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     ms_per_step = ms / args.steps
-    shots_total = len(shots) * world * args.steps
+    n_job = torch.tensor([len(shots)], device=dev)
+    if world > 1:
+        dist.all_reduce(n_job, op=dist.ReduceOp.SUM)
+    shots_total = int(n_job.item()) * args.steps
     value = shots_total / (ms / 1000.0)
     gcell = 2.0 * cells * nt * world * args.steps / (ms / 1000.0) / 1e9
 
@@ -456,34 +456,66 @@ def main():
                d2h_bytes_per_step=int(d2h), api="taichirtm_b200.batch.BatchedRTM.migrate")
     assert np.isfinite(host_img.numpy()).all()
 
-    # the plain path: one shot per launch sequence, same shots, same semantics
-    plain = None
-    if not args.no_plain and rank == 0:
-        nplain = 4
-        t_sum = 0.0
-        shapes = []
+    def plain_rate(nplain, checkpoint=None):
+        """The plain path: shots 0 .. nplain-1 migrated one shot per plan (one
+        shot per launch), same semantics, each plan with its own autotuned
+        launch shape; each timed once after one untimed call."""
+        t_sum, shapes = 0.0, []
         for s in range(nplain):
             sub = [shots[s]]
-            ns = len(sub[0].src)
             o0 = sum(len(x.src) for x in shots[:s])
             r0 = sum(len(x.rec) for x in shots[:s])
             one = BatchedRTM(mu_m, lam_m, rho_m, survey.dx, survey.dz, survey.fs, nt, survey.fw, sub,
                              modes=PSV, tune="auto", device=dev)  # each one-shot plan tuned for itself
             shapes.append({k: v for k, v in one.tune.items() if k != "graphs"})
-            w1 = wav[:, o0:o0 + ns].contiguous()
+            w1 = wav[:, o0:o0 + len(sub[0].src)].contiguous()
             o1 = obs[:, r0:r0 + len(sub[0].rec)].contiguous()
-            one.migrate(w1, o1, isnap=ISNAP)
+            one.migrate(w1, o1, isnap=ISNAP, checkpoint=checkpoint)
             torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            one.migrate(w1, o1, isnap=ISNAP)
+            one.migrate(w1, o1, isnap=ISNAP, checkpoint=checkpoint)
             b.record(stream)
             torch.cuda.synchronize()
             t_sum += a.elapsed_time(b)
             one.close()
-        plain = dict(shots_per_s=round(nplain / (t_sum / 1000.0), 3), launch_shapes=shapes,
-                     sample=f"shots 0..{nplain - 1} migrated one shot per plan (one shot per launch), "
-                            "each plan with its own autotuned launch shape")
+        return dict(shots_per_s=round(nplain / (t_sum / 1000.0), 3), launch_shapes=shapes,
+                    sample=f"shots 0..{nplain - 1} migrated one shot per plan (one shot per launch), "
+                           "each plan with its own autotuned launch shape")
+
+    plain = None
+    if not args.no_plain and rank == 0:
+        plain = plain_rate(4)
+
+    # checkpointed RTM: the same shots with sqrt(nt) checkpoints and the
+    # forward wavefield recomputed segment by segment, batched vs plain
+    ckpt_rtm = None
+    if not args.no_extra and rank == 0:
+        ck = dict(every=max(1, round(nt ** 0.5)), dtype=args.ckpt_dtype or "i16")
+        rtm.migrate(wav, obs, isnap=ISNAP, checkpoint=ck)
+        torch.cuda.synchronize()
+        clk = ClockSampler().start()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(2):
+            ffc, fbc, _ = rtm.migrate(wav, obs, isnap=ISNAP, checkpoint=ck)
+        b.record(stream)
+        torch.cuda.synchronize()
+        cclk = clk.stop()
+        assert int(ffc.max()) == 0 and int(fbc.max()) == 0
+        c_ms = a.elapsed_time(b) / 2
+        c_rate = len(shots) / (c_ms / 1000.0)
+        c_plain = plain_rate(4, checkpoint=ck)
+        ckpt_rtm = dict(shots_per_s=round(c_rate, 3), ms_per_step=round(c_ms, 2), steps=2, warmup=1,
+                        checkpoint=ck, clocks=cclk, plain=c_plain,
+                        batched_vs_plain=round(c_rate / c_plain["shots_per_s"], 2),
+                        workload=workload_desc(len(shots), nt) + f", checkpoints every {ck['every']} steps "
+                                 f"({ck['dtype']}) with recompute instead of snapshots")
+
+    gradient = None
+    if not args.no_extra and rank == 0:
+        from taichirtm_b200 import benchmarks
+        gradient = benchmarks.gradient_leg(nt=3000, steps=3, warmup=1, nplain=2)
 
     cpu = None
     if not args.no_cpu and rank == 0 and world == 1:
@@ -496,16 +528,16 @@ def main():
             metric=METRIC, value=round(value, 4), unit="shots/s", n_gpus=world, steps=args.steps,
             warmup=args.warmup, ms_per_step=round(ms_per_step, 2), higher_is_better=True, scaling="weak",
             vs_baseline=None, dtype="f32", data="synthetic",
-            config=dict(workload=workload_desc(len(shots), nt), shots_per_gpu=len(shots),
-                        cells_per_shot_step=int(cells), grid="2001x801", nt=nt, isnap=ISNAP,
-                        l2="no flush: per-step working set (state 2.6 GB + snapshots 48 GB) >> 126 MB L2",
-                        parallelism=f"shots sharded, {len(shots)} per GPU, FP64 all-reduce of the image",
-                        launch_shape=rtm.tune),
+            config=bench_config(len(base), nt, world, cells), launch_shape=rtm.tune,
             gcell_upd_per_s=round(gcell, 2), roofline=roofline, e2e=e2e,
             gpu_launches=int(launches), clocks=clocks, cpu_baseline=cpu)
         if plain:
             line["plain"] = plain
             line["batched_vs_plain"] = round(value / world / plain["shots_per_s"], 2)
+        if ckpt_rtm:
+            line["checkpointed_rtm"] = ckpt_rtm
+        if gradient:
+            line["gradient"] = gradient
         print(json.dumps(line), flush=True)
     rtm.close()
     if world > 1:

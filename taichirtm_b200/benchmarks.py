@@ -13,7 +13,8 @@ c5  Large batched, checkpointed P-SV RTM plus gradient: 4001 x 1601, dt =
 import json
 import math
 import os
-import time
+import subprocess
+import tempfile
 
 import numpy as np
 import torch
@@ -26,6 +27,57 @@ from .plan import PSV
 
 def _ev():
     return torch.cuda.Event(enable_timing=True)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while a
+    timed region runs (start before it, stop after it)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def stop(self, gpu_index=None):
+        """dict(sm_mhz = median under load, sm_max_mhz, reasons, samples), or
+        None without nvidia-smi.  gpu_index defaults to the first entry of
+        CUDA_VISIBLE_DEVICES."""
+        if self.p is None:
+            return None
+        if gpu_index is None:
+            gpu_index = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0] or None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if gpu_index is not None:
+            sel = [r for r in rows if r[0].strip() == str(gpu_index)]
+            rows = sel or rows
+        if not rows:
+            return None
+        sm = np.array([float(r[1]) for r in rows])
+        mx = max(float(r[2]) for r in rows)
+        pw = np.array([float(r[3]) if r[3].strip() not in ("[N/A]", "N/A") else 0 for r in rows])
+        load = sm[pw > 0.5 * pw.max()] if pw.max() > 0 else sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
+        return dict(sm_mhz=float(np.median(load)), sm_max_mhz=mx, reasons=reasons, samples=len(rows))
 
 
 _ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -107,8 +159,12 @@ def _plain_gradient(sv, shots, wav, obs, m0, K, nt, dev, nplain):
                        "each with its own autotuned launch shape")
 
 
-def run_c4(args):
-    nt = args.nt or 3000
+def gradient_leg(nt=3000, steps=3, warmup=1, nplain=2, with_reference_image=False):
+    """The c4 FWI gradient, timed: 8 shots on the 1201 x 401 model in one
+    problem (every launch advances all shots) against the same gradient one
+    shot per problem (the plain path).  Returns a dict with the batched
+    gradient shots/s, its roofline in compulsory bytes, the plain figure and
+    the clocks of the timed region."""
     sv = S.config4(nt=nt)
     dev = torch.device("cuda")
     shots = survey_shots(sv)
@@ -130,46 +186,64 @@ def run_c4(args):
         J.backward()
         return float(J), [x.grad for x in m]
 
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         J, g = gradient()
     torch.cuda.synchronize()
+    clk = ClockSampler().start()
     e0, e1 = _ev(), _ev()
     e0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         J, g = gradient()
     e1.record()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / steps
     cells = sum(s.nx for s in shots) * sv.nz
-    plain = _plain_gradient(sv, shots, wav, obs, m0, K, nt, dev, nplain=2)
-    # reference backward + imaging (zero-lag cross-correlation) with the data
-    # residual as "observed data": its image vs the exact gradient (reported)
-    rtm = BatchedRTM(*sv.material(migration=True), sv.dx, sv.dz, sv.fs, nt, sv.fw, shots,
-                     tune={k: v for k, v in tune.items() if k != "graphs"}, graphs=False, device=dev)
-    _, syn, _, _ = rtm.forward(wav)
-    resid = (syn - obs).contiguous()
-    _, _, img = rtm.migrate(wav, resid, isnap=5)
-    rtm.close()
-    img = img.cpu().numpy()
-    inner = (slice(sv.fw, sv.nx - sv.fw), slice(5, sv.nz - sv.fw))
-    image_pm = img[0] + img[2]
-    corr = {k: _corr(gk.cpu().numpy()[inner], image_pm[inner]) for k, gk in zip(("vp", "vs", "rho"), g)}
+    plain = _plain_gradient(sv, shots, wav, obs, m0, K, nt, dev, nplain=nplain)
     grad_bytes = 2 * nt * _step_bytes(shots, sv.nz) + 2 * prob.checkpoint_bytes()
     roof = _roofline(grad_bytes, ms, "whole gradient of all shots: 2 phases x nt x (40 B per shot cell + 20 B per "
                                      "model cell under any window) + checkpoints written and read once; the "
                                      "recompute and the gradient sums are not counted; timed end to end per gradient")
-    line = dict(metric="FWI gradient shots/s (P-SV, exact adjoint, sqrt(nt) FP32 checkpoints)",
-                value=round(len(shots) / (ms / 1000.0), 3), unit="shots/s", n_gpus=1, steps=args.steps,
-                warmup=args.warmup, ms_per_step=round(ms, 2), higher_is_better=True, dtype="f32",
-                data="synthetic", config=dict(workload="c4 FWI gradient: 8 shots, 1201x401, dx=5 m, dt=0.5 ms, "
-                                                        f"nt={nt}, L2 misfit on vx and vz, start = smoothed true model (sigma 15)",
-                                               ckpt_every=K, checkpoint_gb=round(prob.checkpoint_bytes() / 1e9, 2),
-                                               launch_shape=dict(rtm=tune, gradient=prob.tune)),
-                gcell_upd_per_s=round(2 * cells * nt / (ms / 1000.0) / 1e9, 2), roofline=roof, misfit=J,
-                plain=plain, batched_vs_plain=round(len(shots) / (ms / 1000.0) / plain["shots_per_s"], 2),
-                normalized_corr_gradient_vs_reference_rtm_image=corr,
-                note="finite-difference (FP64, 10 directions) and dot-product checks: tests/test_gpu_adjoint.py")
+    out = dict(shots_per_s=round(len(shots) / (ms / 1000.0), 3), ms_per_gradient=round(ms, 2),
+               gcell_upd_per_s=round(2 * cells * nt / (ms / 1000.0) / 1e9, 2), roofline=roof, misfit=J,
+               plain=plain, batched_vs_plain=round(len(shots) / (ms / 1000.0) / plain["shots_per_s"], 2),
+               clocks=clocks, steps=steps, warmup=max(1, warmup), ckpt_every=K,
+               checkpoint_gb=round(prob.checkpoint_bytes() / 1e9, 2),
+               launch_shape=dict(rtm=tune, gradient=prob.tune),
+               workload=("c4 FWI gradient: 8 shots, 1201x401, dx=5 m, dt=0.5 ms, "
+                         f"nt={nt}, L2 misfit on vx and vz, start = smoothed true model (sigma 15), "
+                         f"sqrt(nt) = {K}-step FP32 checkpoints with recompute"))
     prob.close()
+    if with_reference_image:
+        # reference backward + imaging (zero-lag cross-correlation) with the data
+        # residual as "observed data": its image vs the exact gradient (reported)
+        rtm = BatchedRTM(*sv.material(migration=True), sv.dx, sv.dz, sv.fs, nt, sv.fw, shots,
+                         tune={k: v for k, v in tune.items() if k != "graphs"}, graphs=False, device=dev)
+        _, syn, _, _ = rtm.forward(wav)
+        resid = (syn - obs).contiguous()
+        _, _, img = rtm.migrate(wav, resid, isnap=5)
+        rtm.close()
+        img = img.cpu().numpy()
+        inner = (slice(sv.fw, sv.nx - sv.fw), slice(5, sv.nz - sv.fw))
+        image_pm = img[0] + img[2]
+        out["normalized_corr_gradient_vs_reference_rtm_image"] = {
+            k: _corr(gk.cpu().numpy()[inner], image_pm[inner]) for k, gk in zip(("vp", "vs", "rho"), g)}
+    return out
+
+
+def run_c4(args):
+    nt = args.nt or 3000
+    r = gradient_leg(nt=nt, steps=args.steps, warmup=args.warmup, with_reference_image=True)
+    line = dict(metric="FWI gradient shots/s (P-SV, exact adjoint, sqrt(nt) FP32 checkpoints)",
+                value=r["shots_per_s"], unit="shots/s", n_gpus=1, steps=args.steps,
+                warmup=r["warmup"], ms_per_step=r["ms_per_gradient"], higher_is_better=True, dtype="f32",
+                data="synthetic", config=dict(workload=r["workload"], ckpt_every=r["ckpt_every"],
+                                               checkpoint_gb=r["checkpoint_gb"]),
+                launch_shape=r["launch_shape"], gcell_upd_per_s=r["gcell_upd_per_s"], roofline=r["roofline"],
+                misfit=r["misfit"], plain=r["plain"], batched_vs_plain=r["batched_vs_plain"], clocks=r["clocks"],
+                normalized_corr_gradient_vs_reference_rtm_image=r["normalized_corr_gradient_vs_reference_rtm_image"],
+                note="finite-difference (FP64) and dot-product checks: tests/test_gpu_adjoint.py, "
+                     "tests/test_gpu_configs_fp64.py")
     print(json.dumps(line), flush=True)
     return 0
 
