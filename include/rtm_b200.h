@@ -170,9 +170,15 @@ size_t rtm_plan_state_floats(const rtm_plan *plan);
 /* Checkpoint slots for interval ckpt_every: ceil(nt / ckpt_every) - 1. */
 int rtm_plan_num_checkpoints(const rtm_plan *plan, int ckpt_every);
 
-/* Checkpoint storage: FP32 (exact), or FP16 / BF16 with one scale per
- * (checkpoint, field, shot): x is stored as round(x * 32752 / max|x|). */
-enum { RTM_CKPT_F32 = 0, RTM_CKPT_F16 = 1, RTM_CKPT_BF16 = 2 };
+/* Checkpoint storage: FP32 (exact), or 16 bits per value with one scale per
+ * block, a block being one row of one shot's field over 60 columns (30 for
+ * plans with vec 1), amax = max |x| over the block:
+ *   RTM_CKPT_F16 / RTM_CKPT_BF16: half / bfloat16 of x * 32752 / amax;
+ *   RTM_CKPT_I16: round(x * 32767 / amax) as int16 (block floating point:
+ *                 15 bits relative to the block maximum, against 11 for F16).
+ * The compressed copy is written by the step launch that produces the
+ * checkpointed state (no extra pass over the wavefield). */
+enum { RTM_CKPT_F32 = 0, RTM_CKPT_F16 = 1, RTM_CKPT_BF16 = 2, RTM_CKPT_I16 = 3 };
 /* Bytes of the checkpoint buffer (data and scale tables) for this interval/dtype. */
 size_t rtm_plan_checkpoint_bytes(const rtm_plan *plan, int ckpt_every, int ckpt_dtype);
 
@@ -180,7 +186,8 @@ size_t rtm_plan_checkpoint_bytes(const rtm_plan *plan, int ckpt_every, int ckpt_
  * also stores the full state after every step it with (it+1) % ckpt_every == 0
  * (rtm_plan_num_checkpoints slots) into ckpt (rtm_plan_checkpoint_bytes).
  * FP32 storage costs no extra traffic (the step writes its output into the
- * slot); FP16/BF16 add an abs-max and a pack pass at checkpoint steps only. */
+ * slot); the 16-bit formats cost the step's extra 10 bytes per cell written
+ * (plus one scale per block) at checkpoint steps only. */
 int rtm_forward_checkpointed(rtm_plan *plan, const float *wavelets, float *seis, int ckpt_every,
                              int ckpt_dtype, void *ckpt, int check_interval, int32_t *flags,
                              rtm_stream_t stream);

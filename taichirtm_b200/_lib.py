@@ -27,7 +27,7 @@ class RtmTune(ctypes.Structure):
 
 
 PSV, SH, BOTH = 1, 2, 3
-CKPT_DTYPES = {"f32": 0, "f16": 1, "bf16": 2}
+CKPT_DTYPES = {"f32": 0, "f16": 1, "bf16": 2, "i16": 3}
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "call out of order", -4: "out of device memory",
           -5: "size above the entry point's limit"}
 

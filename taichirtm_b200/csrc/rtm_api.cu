@@ -306,7 +306,7 @@ cudaError_t launch_mode(const StepParams &sp, int modes, int vec, int warps, cud
     }
 }
 
-template <int DIR, int MODE, int VEC, bool RING, bool STOREA = false>
+template <int DIR, int MODE, int VEC, bool RING, bool STOREA = false, bool CKPT = false>
 cudaError_t launch_step2(const StepParams &sp, int warps, cudaStream_t s) {
     size_t smem = 0;
     if constexpr (RING) {
@@ -316,14 +316,62 @@ cudaError_t launch_step2(const StepParams &sp, int warps, cudaStream_t s) {
         static bool attr_set = false;  // per instantiation; raises the 48 KB default
         if (!attr_set) {
             const size_t want = std::min<size_t>(8 * ring2_smem_per_warp<MODE, VEC>(), kMaxSmem);
-            cudaError_t e = cudaFuncSetAttribute(step2_kernel<DIR, MODE, VEC, RING, STOREA>,
+            cudaError_t e = cudaFuncSetAttribute(step2_kernel<DIR, MODE, VEC, RING, STOREA, CKPT>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
             if (e != cudaSuccess) return e;
             attr_set = true;
         }
     }
-    step2_kernel<DIR, MODE, VEC, RING, STOREA><<<(sp.n_work + warps - 1) / warps, 32 * warps, smem, s>>>(sp);
+    step2_kernel<DIR, MODE, VEC, RING, STOREA, CKPT><<<(sp.n_work + warps - 1) / warps, 32 * warps, smem, s>>>(sp);
     return cudaGetLastError();
+}
+
+// Checkpoint-storing forward P-SV launches (sp.ck set): one step or two
+// steps, the output state also packed into the compressed slot.
+template <int VEC, int PFM>
+cudaError_t launch_step_ckpt(const StepParams &sp, int warps, cudaStream_t s) {
+    const int threads = 32 * warps;
+    const int blocks = (sp.n_work + warps - 1) / warps;
+    size_t smem = 0;
+    if constexpr (PFM == 3) {
+        constexpr size_t kMaxSmem = 227 * 1024;
+        smem = (size_t)warps * async_smem_per_warp<RTM_PSV, VEC>();
+        if (smem > kMaxSmem) return cudaErrorInvalidConfiguration;
+        static bool attr_set = false;
+        if (!attr_set) {
+            const size_t want = std::min<size_t>(8 * async_smem_per_warp<RTM_PSV, VEC>(), kMaxSmem);
+            cudaError_t e = cudaFuncSetAttribute(step_kernel<0, RTM_PSV, VEC, PFM, true>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
+            if (e != cudaSuccess) return e;
+            attr_set = true;
+        }
+    }
+    step_kernel<0, RTM_PSV, VEC, PFM, true><<<blocks, threads, smem, s>>>(sp);
+    return cudaGetLastError();
+}
+template <int VEC>
+cudaError_t launch_pf_ckpt(const StepParams &sp, int pfm, int warps, cudaStream_t s) {
+    switch (pfm) {
+        case 0: return launch_step_ckpt<VEC, 0>(sp, warps, s);
+        case 1: return launch_step_ckpt<VEC, 1>(sp, warps, s);
+        case 2: return launch_step_ckpt<VEC, 2>(sp, warps, s);
+        default: return launch_step_ckpt<VEC, 3>(sp, warps, s);
+    }
+}
+cudaError_t launch_ckpt(const StepParams &sp, bool two, int vec, int prefetch, int warps, cudaStream_t s) {
+    if (two) {
+        const bool ring = prefetch == 3;
+        if (vec == 2)
+            return ring ? launch_step2<0, RTM_PSV, 2, true, false, true>(sp, warps, s)
+                        : launch_step2<0, RTM_PSV, 2, false, false, true>(sp, warps, s);
+        return ring ? launch_step2<0, RTM_PSV, 4, true, false, true>(sp, warps, s)
+                    : launch_step2<0, RTM_PSV, 4, false, false, true>(sp, warps, s);
+    }
+    switch (vec) {
+        case 1: return launch_pf_ckpt<1>(sp, prefetch, warps, s);
+        case 2: return launch_pf_ckpt<2>(sp, prefetch, warps, s);
+        default: return launch_pf_ckpt<4>(sp, prefetch, warps, s);
+    }
 }
 
 template <int DIR, int MODE>
@@ -931,62 +979,67 @@ int rtm_plan_num_checkpoints(const rtm_plan *p, int ckpt_every) {
     return nseg - 1;
 }
 
+static bool ckpt_dtype_ok(int dtype) { return dtype >= RTM_CKPT_F32 && dtype <= RTM_CKPT_I16; }
 static size_t ckpt_elem(int dtype) { return dtype == RTM_CKPT_F32 ? 4 : 2; }
-static size_t ckpt_slot_bytes(const rtm_plan *p, int dtype) {
+static size_t ckpt_data_bytes(const rtm_plan *p, int dtype) {
     return ((size_t)NADJ * p->state_floats * ckpt_elem(dtype) + 255) & ~size_t(255);
 }
-static size_t ckpt_amax_bytes(const rtm_plan *p) { return ((size_t)NADJ * p->nshots * 4 + 255) & ~size_t(255); }
+// Block scales of a compressed slot: one per (field, padded state row, block
+// of ckpt_block_cols(vec) columns).
+static int ckpt_blocks_per_row(const rtm_plan *p) { return p->nstrips * 30 * p->vec / ckpt_block_cols(p->vec); }
+static long long ckpt_scales_per_field(const rtm_plan *p) {
+    return (long long)(p->state_floats / (size_t)p->pitch) * ckpt_blocks_per_row(p);
+}
+static size_t ckpt_scale_bytes(const rtm_plan *p) {
+    return ((size_t)NADJ * (size_t)ckpt_scales_per_field(p) * sizeof(float) + 255) & ~size_t(255);
+}
+static size_t ckpt_slot_total(const rtm_plan *p, int dtype) {
+    return ckpt_data_bytes(p, dtype) + (dtype == RTM_CKPT_F32 ? 0 : ckpt_scale_bytes(p));
+}
 
 size_t rtm_plan_checkpoint_bytes(const rtm_plan *p, int ckpt_every, int ckpt_dtype) {
     const int n = rtm_plan_num_checkpoints(p, ckpt_every);
-    if (n <= 0 || ckpt_dtype < RTM_CKPT_F32 || ckpt_dtype > RTM_CKPT_BF16) return 0;
-    const size_t per = ckpt_slot_bytes(p, ckpt_dtype) + (ckpt_dtype == RTM_CKPT_F32 ? 0 : ckpt_amax_bytes(p));
-    return (size_t)n * per;
+    if (n <= 0 || !ckpt_dtype_ok(ckpt_dtype)) return 0;
+    return (size_t)n * ckpt_slot_total(p, ckpt_dtype);
 }
 
 namespace {
 
-// Checkpoint slot c: data, then (compressed dtypes) its [5][nshots] amax table.
+// Checkpoint slot c: data, then (compressed dtypes) its block-scale table.
 unsigned char *ckpt_slot(const rtm_plan *p, void *ckpt, int dtype, int c) {
-    const size_t per = ckpt_slot_bytes(p, dtype) + (dtype == RTM_CKPT_F32 ? 0 : ckpt_amax_bytes(p));
-    return static_cast<unsigned char *>(ckpt) + (size_t)c * per;
+    return static_cast<unsigned char *>(ckpt) + (size_t)c * ckpt_slot_total(p, dtype);
 }
 
-// Store the 5 FP32 fields `src` into compressed slot c (absmax, then pack).
-int ckpt_store(rtm_plan *p, void *ckpt, int dtype, int c, float *const *src, cudaStream_t s) {
+// The compressed slot c as the storing step launch writes it.
+CkptOut ckpt_out(const rtm_plan *p, void *ckpt, int dtype, int c) {
     unsigned char *slot = ckpt_slot(p, ckpt, dtype, c);
-    CkptParams cp{};
-    for (int f = 0; f < NADJ; ++f) cp.src[f] = src[f];
-    cp.half = slot;
-    cp.amax = reinterpret_cast<unsigned int *>(slot + ckpt_slot_bytes(p, dtype));
-    cp.shots = p->d_shots;
-    cp.nshots = p->nshots;
-    cp.pitch = p->pitch;
-    cp.sf = p->state_floats;
-    CUDA_TRY(cudaMemsetAsync(cp.amax, 0, (size_t)NADJ * p->nshots * 4, s));
-    dim3 grid(64, p->nshots, NADJ);
-    ckpt_absmax_kernel<<<grid, 256, 0, s>>>(cp);
-    CUDA_TRY(cudaGetLastError());
-    if (dtype == RTM_CKPT_F16) ckpt_pack_kernel<__half><<<grid, 256, 0, s>>>(cp);
-    else ckpt_pack_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>(cp);
-    CUDA_TRY(cudaGetLastError());
-    return 0;
+    CkptOut o{};
+    o.data = slot;
+    o.scale = reinterpret_cast<float *>(slot + ckpt_data_bytes(p, dtype));
+    o.field_elems = (long long)p->state_floats;
+    o.scale_per_field = ckpt_scales_per_field(p);
+    o.dtype = dtype;
+    o.nblk = ckpt_blocks_per_row(p);
+    return o;
 }
 
-// Restore compressed slot c into the 5 FP32 fields `dst`.
+// Restore compressed slot c into the 5 FP32 fields `dst` (their pad rows and
+// pad columns are left as they are: zero).
 int ckpt_load(rtm_plan *p, const void *ckpt, int dtype, int c, float *const *dst, cudaStream_t s) {
-    unsigned char *slot = ckpt_slot(p, const_cast<void *>(ckpt), dtype, c);
-    CkptParams cp{};
-    for (int f = 0; f < NADJ; ++f) cp.dst[f] = dst[f];
-    cp.half = slot;
-    cp.amax = reinterpret_cast<unsigned int *>(slot + ckpt_slot_bytes(p, dtype));
-    cp.shots = p->d_shots;
-    cp.nshots = p->nshots;
-    cp.pitch = p->pitch;
-    cp.sf = p->state_floats;
-    dim3 grid(64, p->nshots, NADJ);
-    if (dtype == RTM_CKPT_F16) ckpt_unpack_kernel<__half><<<grid, 256, 0, s>>>(cp);
-    else ckpt_unpack_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>(cp);
+    const CkptOut o = ckpt_out(p, const_cast<void *>(ckpt), dtype, c);
+    CkptIn ci{};
+    ci.data = o.data;
+    ci.scale = o.scale;
+    for (int f = 0; f < NADJ; ++f) ci.dst[f] = dst[f];
+    ci.field_elems = o.field_elems;
+    ci.scale_per_field = o.scale_per_field;
+    ci.shots = p->d_shots;
+    ci.pitch = p->pitch;
+    ci.ncols = p->nstrips * 30 * p->vec;
+    ci.nblk = ckpt_blocks_per_row(p);
+    ci.block_w = ckpt_block_cols(p->vec);
+    ci.dtype = dtype;
+    ckpt_unpack_kernel<<<dim3(64, p->nshots, NADJ), 256, 0, s>>>(ci);
     CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -1019,7 +1072,7 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
     if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
     if (p->g.modes != RTM_PSV) return fail(RTM_E_ARG, "checkpointed propagation supports the P-SV mode");
     if (ckpt_every <= 0) return fail(RTM_E_ARG, "ckpt_every must be positive");
-    if (ckpt_dtype < RTM_CKPT_F32 || ckpt_dtype > RTM_CKPT_BF16) return fail(RTM_E_ARG, "bad ckpt_dtype");
+    if (!ckpt_dtype_ok(ckpt_dtype)) return fail(RTM_E_ARG, "bad ckpt_dtype");
     if (p->nsrc_total > 0 && !wavelets) return fail(RTM_E_ARG, "null wavelets");
     const int nt = p->g.nt;
     const int nck = rtm_plan_num_checkpoints(p, ckpt_every);
@@ -1032,8 +1085,9 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
     bs.add(ckpt, rtm_plan_checkpoint_bytes(p, ckpt_every, ckpt_dtype));
     if (int rc = bs.begin(s)) return rc;
     if (int rc = zero_state(p, s)) return rc;
-    if (nck > 0 && ckpt_dtype == RTM_CKPT_F32)
-        CUDA_TRY(cudaMemsetAsync(ckpt, 0, rtm_plan_checkpoint_bytes(p, ckpt_every, ckpt_dtype), s));
+    // every slot starts at zero: pad rows / columns of FP32 slots, and the
+    // slots of a shot that stops before reaching them
+    if (nck > 0) CUDA_TRY(cudaMemsetAsync(ckpt, 0, rtm_plan_checkpoint_bytes(p, ckpt_every, ckpt_dtype), s));
     const size_t nseis = (size_t)3 * nt * p->nrec_total;
     if (nseis) CUDA_TRY(cudaMemsetAsync(p->d_seis_t, 0, nseis * sizeof(float), s));
     StepParams sp;
@@ -1069,15 +1123,18 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
         if (ln.two) {
             sp.it2 = last;
             sp.snap_k2 = -1;
+        }
+        if (save && ckpt_dtype != RTM_CKPT_F32) {
+            // the launch also packs its output state into compressed slot c
+            sp.ck = ckpt_out(p, ckpt, ckpt_dtype, c);
+            CUDA_TRY(launch_ckpt(sp, ln.two, p->vec, p->prefetch, p->warps, s));
+            sp.ck = CkptOut{};
+        } else if (ln.two) {
             CUDA_TRY((launch_mode2<0>(sp, p->g.modes, p->vec, p->prefetch, p->warps, s)));
         } else {
             CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, s)));
         }
         ++p->launches;
-        if (save && ckpt_dtype != RTM_CKPT_F32) {
-            if (int rc = ckpt_store(p, ckpt, ckpt_dtype, c, out, s)) return rc;
-            p->launches += 2;
-        }
         for (int f = 0; f < NADJ; ++f) in[f] = out[f];
     }
     if (seis && p->nrec_total) {
@@ -1099,7 +1156,7 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
     if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
     if (p->g.modes != RTM_PSV) return fail(RTM_E_ARG, "the adjoint supports the P-SV mode");
     if (ckpt_every <= 0) return fail(RTM_E_ARG, "ckpt_every must be positive");
-    if (ckpt_dtype < RTM_CKPT_F32 || ckpt_dtype > RTM_CKPT_BF16) return fail(RTM_E_ARG, "bad ckpt_dtype");
+    if (!ckpt_dtype_ok(ckpt_dtype)) return fail(RTM_E_ARG, "bad ckpt_dtype");
     if (!grad) return fail(RTM_E_ARG, "null gradient output");
     if (p->nrec_total > 0 && !resid) return fail(RTM_E_ARG, "null residual");
     if (p->nsrc_total > 0 && !wavelets) return fail(RTM_E_ARG, "null wavelets");
@@ -1294,7 +1351,7 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
     if (!p->model_set) return fail(RTM_E_STATE, "rtm_plan_set_model has not been called");
     if (p->g.modes != RTM_PSV) return fail(RTM_E_ARG, "checkpointed RTM supports the P-SV mode");
     if (ckpt_every <= 0 || isnap <= 0) return fail(RTM_E_ARG, "ckpt_every and isnap must be positive");
-    if (ckpt_dtype < RTM_CKPT_F32 || ckpt_dtype > RTM_CKPT_BF16) return fail(RTM_E_ARG, "bad ckpt_dtype");
+    if (!ckpt_dtype_ok(ckpt_dtype)) return fail(RTM_E_ARG, "bad ckpt_dtype");
     if (p->nrec_total > 0 && !obs) return fail(RTM_E_ARG, "null observed data");
     if (p->nsrc_total > 0 && !wavelets) return fail(RTM_E_ARG, "null wavelets");
     if (image && p->nshots != 1) return fail(RTM_E_ARG, "image output needs a single-shot plan; use stack");

@@ -97,10 +97,13 @@ __host__ __device__ constexpr size_t ring2_smem_per_warp() {
 
 // STOREA: also store step A's state (rows [ia, ib), into p.souta), for the
 // forward recompute of the FWI adjoint, which needs the state after every step.
-template <int DIR, int MODE, int VEC, bool RING = false, bool STOREA = false>
+// CKPT: step B's state is also stored, block-scaled to 16 bits, into the
+// checkpoint slot p.ck (ckpt_pack.cuh); forward P-SV only.
+template <int DIR, int MODE, int VEC, bool RING = false, bool STOREA = false, bool CKPT = false>
 __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     static_assert(VEC >= 2, "two steps per launch need two halo columns per side");
     static_assert(!STOREA || DIR == 0, "only the forward recompute stores step A");
+    static_assert(!CKPT || (DIR == 0 && MODE == 1), "checkpoint stores are forward P-SV");
     constexpr bool PSV = (MODE & 1) != 0;
     constexpr bool SH = (MODE & 2) != 0;
     constexpr int W = 30 * VEC;
@@ -130,6 +133,9 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     const long long moff = (long long)sh.x0 * P + (long long)(c0 + COL_OFF);
     const float dt = p.dt, idx = p.inv_dx, idz = p.inv_dz;
     const float sdt = DIR == 0 ? dt : -dt;
+    // CKPT: scale block of row -1 of this task's strip (padded row 0 of the shot)
+    long long ck_blk0 = 0;
+    if constexpr (CKPT) ck_blk0 = (sh.state_off / P) * p.ck.nblk + (wk.y & 0xFFFFF) * (W / ckpt_block_cols(VEC));
     // rows -1 and nx are the zero pad rows of the shot block (and of the
     // material window); rows beyond them read the pad row (header comment)
     auto rowc = [&](int i) { return min(max(i, -1), nx); };
@@ -511,6 +517,9 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     (void)store_a;
     // step B's stress and absorbed velocity of row r: store, outputs, check
     auto finish_b = [&](int r, const Sig &os, const Vel &ov) {
+        if constexpr (CKPT)
+            ckpt_pack_row<VEC>(p.ck, soff + (long long)(r + 1) * P, ck_blk0 + (long long)(r + 1) * p.ck.nblk, lane,
+                               owner, ov.u, ov.w, os.xx, os.zz, os.xz);
         if (!owner) return;
         const long long so = soff + (long long)(r + 1) * P;
         if constexpr (PSV) {

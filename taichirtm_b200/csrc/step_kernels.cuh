@@ -41,6 +41,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "ckpt_pack.cuh"
 #include "debug_bounds.cuh"
 
 namespace rtm {
@@ -90,6 +91,7 @@ struct StepParams {
     int it;                  // forward: step it; backward: reversed time t
     int it2, snap_k2;        // two-step launches: time and snapshot slot of the second step
     float *souta[NFIELD];    // two-step launches storing the first step's state too (recompute)
+    CkptOut ck;              // CKPT launches: the compressed checkpoint slot of the output state
 };
 
 template <int VEC>
@@ -246,8 +248,11 @@ __device__ __forceinline__ void kahan_add(float &sum, float &comp, float prod) {
 // ASYNC_DEPTH-1 ahead copied by cp.async into a per-warp shared-memory ring;
 // launch with async_smem_per_warp() bytes of dynamic shared memory per warp).
 // None of them changes a result bit.
-template <int DIR, int MODE, int VEC, int PFM = 0>
+// CKPT (forward P-SV only): the launch's output state is also stored, block-
+// scaled to 16 bits, into the checkpoint slot p.ck (ckpt_pack.cuh).
+template <int DIR, int MODE, int VEC, int PFM = 0, bool CKPT = false>
 __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
+    static_assert(!CKPT || (DIR == 0 && MODE == 1), "checkpoint stores are forward P-SV");
     constexpr bool PF = PFM == 1 || PFM == 2;
     constexpr bool HINT = PFM == 2;
     constexpr bool ASYNC = PFM == 3;
@@ -293,6 +298,9 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
     const long long moff = (long long)sh.x0 * P + (long long)(c0 + COL_OFF);
     const float dt = p.dt, idx = p.inv_dx, idz = p.inv_dz;
     const float sdt = DIR == 0 ? dt : -dt;
+    // CKPT: scale block of row -1 of this task's strip (padded row 0 of the shot)
+    long long ck_blk0 = 0;
+    if constexpr (CKPT) ck_blk0 = (sh.state_off / P) * p.ck.nblk + (wk.y & 0xFFFFF) * (W / ckpt_block_cols(VEC));
     auto S = [&](int f, int i) { return p.sin[f] + soff + (long long)(i + 1) * P; };
     auto M = [&](int m, int i) { return p.mat[m] + moff + (long long)(i + 1) * P; };
 
@@ -491,6 +499,9 @@ __global__ void __launch_bounds__(256) step_kernel(const StepParams p) {
                 o_v[q] = cr[q] * va_v[q];
             }
         }
+        if constexpr (CKPT)
+            ckpt_pack_row<VEC>(p.ck, soff + (long long)(r + 1) * P, ck_blk0 + (long long)(r + 1) * p.ck.nblk, lane,
+                               owner, o_u, o_w, o_sxx, o_szz, o_sxz);
         if (!owner) return;
         const long long so = soff + (long long)(r + 1) * P;
         if constexpr (PSV) {

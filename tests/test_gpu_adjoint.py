@@ -255,7 +255,8 @@ def _windowed_case(nt=200, seed=9):
 
 def test_checkpointed_rtm_equals_snapshot_rtm_and_compressed_error():
     """FP32 checkpoints + recompute give the snapshot path's image bit for bit;
-    FP16 / BF16 per-field-scaled checkpoints stay close (errors printed)."""
+    the block-scaled 16-bit checkpoints stay close (errors printed), the
+    int16 block-floating-point format closest."""
     from taichirtm_b200.batch import BatchedRTM
     C = _windowed_case()
     kw = dict(tune=dict(vec=2, rows=16, warps=4), graphs=False)
@@ -269,11 +270,12 @@ def test_checkpointed_rtm_equals_snapshot_rtm_and_compressed_error():
         _, _, st = rtm.migrate(C["wav"], obs, isnap=4, checkpoint=dict(every=every, dtype="f32"))
         assert np.array_equal(st.cpu().numpy(), ref), every
     errs = {}
-    for dt in ("f16", "bf16"):
+    for dt in ("f16", "bf16", "i16"):
         _, _, st = rtm.migrate(C["wav"], obs, isnap=4, checkpoint=dict(every=13, dtype=dt))
         errs[dt] = rel_l2(st.cpu().numpy()[[0, 2]], ref[[0, 2]])
     print("compressed-checkpoint image rel-L2:", errs)
-    assert errs["f16"] < 5e-3 and errs["bf16"] < 5e-2, errs
+    assert errs["f16"] < 5e-3 and errs["bf16"] < 5e-2 and errs["i16"] < 1e-4, errs
+    assert errs["i16"] < 0.25 * errs["f16"], errs
     rtm.close()
 
 
@@ -283,7 +285,7 @@ def test_compressed_checkpoint_gradient_error():
     lam, mu, rho = (torch.as_tensor(x, dtype=torch.float32) for x in _lame(P["vp"], P["vs"], P["rho"]))
     rng = np.random.default_rng(11)
     out = {}
-    for dt in ("f32", "f16", "bf16"):
+    for dt in ("f32", "f16", "bf16", "i16"):
         prob = _fwi(P, ckpt=16)
         prob = FWIProblem(P["nx"], P["nz"], P["dx"], P["dz"], P["fs"], P["nt"], P["fw"],
                           prob.plan.shots, P["wav"], ckpt_every=16, ckpt_dtype=dt)
@@ -294,8 +296,35 @@ def test_compressed_checkpoint_gradient_error():
         prob.close()
     e16 = rel_l2(out["f16"], out["f32"])
     eb16 = rel_l2(out["bf16"], out["f32"])
-    print("compressed-checkpoint gradient rel-L2: f16 %.2e bf16 %.2e" % (e16, eb16))
-    assert e16 < 1e-2 and eb16 < 1e-1
+    ei16 = rel_l2(out["i16"], out["f32"])
+    print("compressed-checkpoint gradient rel-L2: f16 %.2e bf16 %.2e i16 %.2e" % (e16, eb16, ei16))
+    assert e16 < 1e-2 and eb16 < 1e-1 and ei16 < 1e-4
+    assert ei16 < 0.25 * e16
+
+
+@pytest.mark.parametrize("dtype", ["f16", "i16"])
+def test_compressed_checkpoints_independent_of_launch_shape(dtype):
+    """The 16-bit checkpoints are scaled per 60-column block whatever the
+    warp strip (60 columns at vec 2, 120 at vec 4), and written by the step
+    launch that produces the state (one or two steps per launch): the
+    gradient is bit-identical across these launch shapes."""
+    from taichirtm_b200.fwi import FWIProblem
+    from taichirtm_b200.plan import ShotGeometry
+    P = _problem(nt=150)
+    lam, mu, rho = _lame(P["vp"], P["vs"], P["rho"])
+    grads = []
+    for tune in (dict(vec=2, rows=8, warps=2, tsteps=1), dict(vec=2, rows=6, warps=2, tsteps=2, prefetch=3),
+                 dict(vec=4, rows=5, warps=1, prefetch=1), dict(vec=4, rows=7, warps=2, tsteps=2)):
+        prob = FWIProblem(P["nx"], P["nz"], P["dx"], P["dz"], P["fs"], P["nt"], P["fw"],
+                          [ShotGeometry(0, P["nx"], P["src"], P["rec"])], P["wav"], ckpt_every=12, tune=tune,
+                          ckpt_dtype=dtype)
+        seis, ck, _ = prob.forward(lam, mu, rho)
+        g, _ = prob.adjoint(seis * 0.3, ck)
+        grads.append(g.cpu().numpy())
+        prob.close()
+    assert np.abs(grads[0]).max() > 0
+    for g in grads[1:]:
+        assert np.array_equal(grads[0], g)
 
 
 def test_gradient_independent_of_launch_shape_and_autotuned():

@@ -150,7 +150,8 @@ def _batched(tsteps, checkpoint=None, modes=1):
     return res
 
 
-@pytest.mark.parametrize("checkpoint", [None, dict(every=8, dtype="f32"), dict(every=7, dtype="f16")])
+@pytest.mark.parametrize("checkpoint", [None, dict(every=8, dtype="f32"), dict(every=7, dtype="f16"),
+                                        dict(every=7, dtype="i16")])
 def test_two_steps_batched_windows_and_checkpointed(checkpoint):
     a = _batched(1, checkpoint)
     b = _batched(2, checkpoint)
