@@ -39,7 +39,8 @@ enum {
     RTM_E_CUDA = -2,     /* a CUDA runtime call failed (see rtm_last_error) */
     RTM_E_STATE = -3,    /* call out of order (e.g. propagate before set_model) */
     RTM_E_NOMEM = -4,    /* device allocation failed */
-    RTM_E_RANGE = -5     /* size above a fixed limit of the entry point */
+    RTM_E_RANGE = -5,    /* size above a fixed limit of the entry point */
+    RTM_E_CALLBACK = -6  /* the step callback (rtm_plan_set_callback) asked to stop */
 };
 
 enum { RTM_PSV = 1, RTM_SH = 2, RTM_BOTH = 3 };
@@ -252,6 +253,29 @@ int rtm_noalloc_prepare(void);
 size_t rtm_noalloc_scratch_bytes(void);
 size_t rtm_noalloc_required_bytes(const rtm_grid *grid, int nsrc, int nrec);
 const char *rtm_noalloc_last_error(void);
+
+/* Host step callback of rtm_forward and rtm_backward: the display_callback
+ * of ForwardModeling.run (forward_modeling.py:553-559) and
+ * BackwardModeling.run_calc (backward_modeling.py:565-569).  With a callback
+ * set, rtm_forward calls cb(user, it) after step it for every it with
+ * it % forward_every == 0 (it = 0 included), and rtm_backward calls cb(user, t)
+ * after every imaging step t (t > 0, t % isnap == 0, a matching snapshot),
+ * after its correlation -- the reference's steps and order.  Each call comes
+ * after the stream has finished that step; rtm_plan_wavefield then gives the
+ * live wavefield.  As in the reference, no callback follows a failed finite
+ * check (the one at the failing step itself is made: the reference calls
+ * back before it checks).  A non-zero return stops the loop: the entry
+ * point returns RTM_E_CALLBACK.  The time loop then runs as direct launches
+ * (no CUDA-graph replay) that end at every callback step.  cb = NULL clears
+ * it.  No reference counterpart as a C function. */
+typedef int (*rtm_step_callback)(void *user, int step);
+int rtm_plan_set_callback(rtm_plan *plan, int forward_every, rtm_step_callback cb, void *user);
+/* The velocity wavefield of one shot as the last step of rtm_forward /
+ * rtm_backward left it (during a step callback: after that step), copied to
+ * dense (nx_shot, nz) DEVICE arrays u, v, w (any may be NULL; a component the
+ * plan does not propagate is written as zeros).  RTM_E_STATE before any
+ * rtm_forward / rtm_backward, or after a checkpointed entry point. */
+int rtm_plan_wavefield(const rtm_plan *plan, int shot, float *u, float *v, float *w, rtm_stream_t stream);
 
 /* Diagnostics: kernels launched by the last propagate call, and the last
  * error message of this thread. */

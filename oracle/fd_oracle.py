@@ -232,7 +232,7 @@ class Propagator:
 
 def forward(mu, lam, rho, dx, dz, nt, fs, fw, src, wu, wv, ww, rec, isnap=10,
             surface=None, save=False, check_interval=100, dtype=np.float64,
-            return_state=False, setup_f64=False):
+            return_state=False, setup_f64=False, display_callback=None):
     """ForwardModeling.run, forward_modeling.py:504-575.
 
     Returns dict(flag, seis (3, nrec, nt), snaps (3, nx, nz, nsnap) or None,
@@ -240,7 +240,9 @@ def forward(mu, lam, rho, dx, dz, nt, fs, fw, src, wu, wv, ww, rec, isnap=10,
     like the reference (the seismogram is filled up to that step).
     ``check_interval=0`` disables the finite check (used to compare with the
     Taichi-stub golden runs, whose check cannot fire).  ``setup_f64`` evaluates
-    the one-time material set-up in FP64 (see Propagator)."""
+    the one-time material set-up in FP64 (see Propagator).
+    ``display_callback(u, v, w, it)`` gets copies of the wavefield at every
+    it % isnap == 0, before that step's finite check (forward_modeling.py:553-559)."""
     p = Propagator(mu, lam, rho, dx, dz, fs, fw, surface, dtype, setup_f64)
     src = np.asarray(src).reshape(-1, 2)
     rec = np.asarray(rec).reshape(-1, 2)
@@ -264,6 +266,8 @@ def forward(mu, lam, rho, dx, dz, nt, fs, fw, src, wu, wv, ww, rec, isnap=10,
         seis[0, :, it] = p.s.u[ri, rj]
         seis[1, :, it] = p.s.v[ri, rj]
         seis[2, :, it] = p.s.w[ri, rj]
+        if display_callback is not None and it % isnap == 0:
+            display_callback(p.s.u.copy(), p.s.v.copy(), p.s.w.copy(), it)
         if check_interval and it % check_interval == 0:
             flag = p.check_finite(1)
             if flag:
@@ -284,12 +288,14 @@ def forward(mu, lam, rho, dx, dz, nt, fs, fw, src, wu, wv, ww, rec, isnap=10,
 
 def backward(mu, lam, rho, dx, dz, nt, fs, fw, rec, ou, ov, ow, snaps, isnaps, num_snaps,
              isnap, surface=None, check_interval=100, dtype=np.float64, return_state=False,
-             setup_f64=False, kahan=False):
+             setup_f64=False, kahan=False, display_callback=None):
     """BackwardModeling.run_calc, backward_modeling.py:498-579.
 
     ``snaps`` is (3, nx, nz, nsnap) like the reference's snapshot fields.
     ``kahan`` accumulates the image with Kahan compensation (sum, comp) and
     returns sum - comp evaluated in FP64 then rounded to ``dtype``.
+    ``display_callback(u, v, w, t)`` gets copies of the backward wavefield
+    after every imaging step (backward_modeling.py:565-569).
     Returns dict(flag, img (3, nx, nz))."""
     p = Propagator(mu, lam, rho, dx, dz, fs, fw, surface, dtype, setup_f64)
     comp = np.zeros((3, p.nx, p.nz), dtype)
@@ -316,6 +322,8 @@ def backward(mu, lam, rho, dx, dz, nt, fs, fw, rec, ou, ov, ow, snaps, isnaps, n
                         img[c] = tot
                     else:
                         img[c] += prod
+                if display_callback is not None:
+                    display_callback(p.s.u.copy(), p.s.v.copy(), p.s.w.copy(), t)
         if check_interval and it % check_interval == 0:
             flag = p.check_finite(4)
             if flag:

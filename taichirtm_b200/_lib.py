@@ -8,6 +8,8 @@ import os
 from . import build as _build
 
 I32P = ctypes.POINTER(ctypes.c_int32)
+# rtm_step_callback: int (*)(void *user, int step)
+STEP_CALLBACK = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int)
 
 
 class RtmGrid(ctypes.Structure):
@@ -29,7 +31,7 @@ class RtmTune(ctypes.Structure):
 PSV, SH, BOTH = 1, 2, 3
 CKPT_DTYPES = {"f32": 0, "f16": 1, "bf16": 2, "i16": 3}
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "call out of order", -4: "out of device memory",
-          -5: "size above the entry point's limit"}
+          -5: "size above the entry point's limit", -6: "stopped by the step callback"}
 
 _lib = None
 
@@ -82,6 +84,8 @@ def lib():
     _sig(L, "rtm_forward_checkpointed", c_int, vp, vp, vp, c_int, c_int, vp, c_int, I32P, vp)
     _sig(L, "rtm_adjoint", c_int, vp, vp, vp, c_int, c_int, vp, vp, vp, vp)
     _sig(L, "rtm_backward_checkpointed", c_int, vp, vp, vp, c_int, c_int, vp, c_int, vp, vp, c_int, I32P, vp)
+    _sig(L, "rtm_plan_set_callback", c_int, vp, c_int, STEP_CALLBACK, vp)
+    _sig(L, "rtm_plan_wavefield", c_int, vp, c_int, vp, vp, vp, vp)
     for name, args in _OPTIONAL.items():
         if hasattr(L, name):
             _sig(L, name, *args)

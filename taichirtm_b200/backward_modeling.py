@@ -6,7 +6,7 @@ import numpy as np
 import torch
 
 from .fields import DeviceField, to_numpy, to_tensor
-from .forward_modeling import material_is_regular, pick_modes
+from .forward_modeling import material_is_regular, pick_modes, run_with_display
 from .plan import PSV, SH, Plan, ShotGeometry, require_cuda
 
 
@@ -104,14 +104,18 @@ class BackwardModeling:
         isnaps = to_numpy(isnaps_field, np.int32).reshape(-1)[: max(int(num_snaps), 0)]
         snaps = self._snapshot_buffers((import_fwdata_u, import_fwdata_v, import_fwdata_w), int(num_snaps))
         eps = float(normalization_eps) if method == "source_normalized" else None
-        flags, img, _ = self.plan.backward(self._obs, snaps, isnaps, int(num_snaps), int(isnap_interval),
-                                           check_interval=stability_check_interval, image=True,
-                                           normalize_eps=eps)
-        self._img = img
-        if display_callback is not None:
-            im = img.cpu().numpy()
-            display_callback(im[0], im[1], im[2], 0, self.nx, self.nz, self.dx, self.dz)
-        return int(flags[0])
+
+        def run():
+            flags, img, _ = self.plan.backward(self._obs, snaps, isnaps, int(num_snaps), int(isnap_interval),
+                                               check_interval=stability_check_interval, image=True,
+                                               normalize_eps=eps)
+            self._img = img
+            return int(flags[0])
+        if display_callback is None:
+            return run()
+        # like the reference (backward_modeling.py:565-569): the live backward
+        # wavefield after every imaging step, with its time t
+        return run_with_display(self.plan, 0, display_callback, self.dx, self.dz, run)
 
     def get_results(self) -> tuple:
         """(image_u, image_v, image_w), each (nx, nz) float32 NumPy."""

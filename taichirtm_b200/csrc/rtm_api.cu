@@ -109,6 +109,12 @@ struct rtm_plan {
     cudaStream_t gstream = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
     GraphCache g_fwd, g_bwd, g_ckpt;
+    // Host step callback (rtm_plan_set_callback) and the ping-pong buffer that
+    // holds the latest state of rtm_forward / rtm_backward (-1: none).
+    rtm_step_callback cb = nullptr;
+    void *cb_user = nullptr;
+    int cb_every = 0;
+    int live = -1;
 };
 
 namespace {
@@ -420,6 +426,22 @@ std::vector<LoopLaunch> loop_schedule(int first, int end, int tsteps, Pairable &
     return out;
 }
 
+// The host callback after launch number `seq` (1-based) at step `step`:
+// waits for the stream, skips the call once every shot stopped in an earlier
+// launch (a failed check ends the reference's loop before its next
+// callback), and turns a non-zero return into RTM_E_CALLBACK.
+int call_back(rtm_plan *p, int seq, int step, cudaStream_t s) {
+    CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<int> fs(p->nshots);
+    CUDA_TRY(cudaMemcpy(fs.data(), p->d_fail_seq, p->nshots * sizeof(int), cudaMemcpyDeviceToHost));
+    bool alive = false;
+    for (int v : fs) alive = alive || v >= seq;
+    if (!alive) return 0;
+    if (int rc = p->cb(p->cb_user, step))
+        return fail(RTM_E_CALLBACK, "the step callback returned %d at step %d", rc, step);
+    return 0;
+}
+
 void fill_common(const rtm_plan *p, StepParams &sp) {
     std::memset(&sp, 0, sizeof sp);
     const double dt = 1.0 / p->g.fs;
@@ -670,6 +692,38 @@ size_t rtm_plan_snapshot_floats(const rtm_plan *p, int nsnap) {
 
 long long rtm_plan_launch_count(const rtm_plan *p) { return p ? p->launches : 0; }
 
+int rtm_plan_set_callback(rtm_plan *p, int forward_every, rtm_step_callback cb, void *user) {
+    if (!p) return fail(RTM_E_ARG, "null plan");
+    if (cb && forward_every < 0) return fail(RTM_E_ARG, "forward_every < 0");
+    p->cb = cb;
+    p->cb_user = cb ? user : nullptr;
+    p->cb_every = cb ? forward_every : 0;
+    return RTM_OK;
+}
+
+int rtm_plan_wavefield(const rtm_plan *p, int shot, float *u, float *v, float *w, rtm_stream_t stream) {
+    if (!p) return fail(RTM_E_ARG, "null plan");
+    if (shot < 0 || shot >= p->nshots) return fail(RTM_E_ARG, "shot %d outside [0, %d)", shot, p->nshots);
+    if (p->live < 0) return fail(RTM_E_STATE, "no wavefield: rtm_forward / rtm_backward has not run");
+    cudaStream_t s = (cudaStream_t)stream;
+    const ShotDev &d = p->shots_h[shot];
+    const int nz = p->g.nz;
+    float *dst[3] = {u, v, w};
+    const int field[3] = {F_U, F_V, F_W};
+    for (int c = 0; c < 3; ++c) {
+        if (!dst[c]) continue;
+        const float *src = p->d_state[p->live][field[c]];
+        if (!src) {  // a mode the plan does not propagate: zero
+            CUDA_TRY(cudaMemsetAsync(dst[c], 0, (size_t)d.nx * nz * sizeof(float), s));
+            continue;
+        }
+        CUDA_TRY(cudaMemcpy2DAsync(dst[c], (size_t)nz * sizeof(float), src + d.state_off + p->pitch + COL_OFF,
+                                   (size_t)p->pitch * sizeof(float), (size_t)nz * sizeof(float), (size_t)d.nx,
+                                   cudaMemcpyDeviceToDevice, s));
+    }
+    return RTM_OK;
+}
+
 int rtm_plan_set_model(rtm_plan *p, const float *mu, const float *lam, const float *rho,
                        const float *surface, rtm_stream_t stream) {
     NvtxRange nvtx_range("rtm_plan_set_model");
@@ -760,7 +814,11 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
         const int k = (save && it % isnap == 0 && it != 0) ? it / isnap - 1 : -1;  // fm:569-570
         return k < nsnap ? k : -1;
     };
-    const std::vector<LoopLaunch> sched = loop_schedule(0, nt, p->tsteps, [&](int it) { return !check_at(it); });
+    // display_callback steps, it % every == 0 (forward_modeling.py:553-559):
+    // a launch ends at each of them
+    auto cb_at = [&](int it) { return p->cb && p->cb_every > 0 && it % p->cb_every == 0; };
+    const std::vector<LoopLaunch> sched =
+        loop_schedule(0, nt, p->tsteps, [&](int it) { return !check_at(it) && !cb_at(it); });
     auto loop = [&](cudaStream_t ls) -> int {
         for (size_t L = 0; L < sched.size(); ++L) {
             const int it = sched[L].it;
@@ -771,6 +829,7 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
             sp.it = it;
             sp.seq = it + 1;
             sp.snap_k = snap_at(it);
+            const int last = sched[L].two ? it + 1 : it;
             if (sched[L].two) {
                 sp.it2 = it + 1;
                 sp.snap_k2 = snap_at(it + 1);
@@ -780,13 +839,21 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
                 sp.check = check_at(it);
                 CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, ls)));
             }
+            p->live = (int)((L + 1) & 1);
+            if (cb_at(last))
+                if (int rc = call_back(p, it + 1, last, ls)) return rc;
         }
         return 0;
     };
     const std::vector<unsigned long long> key = {U(wavelets), U(snap_u), U(snap_v), U(snap_w),
                                                  (unsigned long long)save, (unsigned long long)isnap,
                                                  (unsigned long long)check_interval};
-    if (int rc = run_loop(p, p->g_fwd, key, s, loop)) return rc;
+    if (p->cb) {  // host callbacks in the loop: direct launches
+        if (int rc = loop(s)) return rc;
+    } else if (int rc = run_loop(p, p->g_fwd, key, s, loop)) {
+        return rc;
+    }
+    p->live = (int)(sched.size() & 1);  // also when a replayed graph ran the loop
     p->launches += (long long)sched.size();
     if (seis && p->nrec_total) {
         if (int rc = transpose(p->d_seis_t, seis, 3, nt, p->nrec_total, s)) return rc;
@@ -864,7 +931,11 @@ static int backward_impl(rtm_plan *p, const float *obs, const float *snap_u, con
         }
     }
     auto check_at = [&](int it) { return check_interval > 0 && it % check_interval == 0; };
-    const std::vector<LoopLaunch> sched = loop_schedule(0, nt, p->tsteps, [&](int it) { return !check_at(it); });
+    // display_callback at every imaging step, after the correlation
+    // (backward_modeling.py:565-569): a launch ends at each of them
+    auto cb_at = [&](int it) { return p->cb && snap_of[it] >= 0; };
+    const std::vector<LoopLaunch> sched =
+        loop_schedule(0, nt, p->tsteps, [&](int it) { return !check_at(it) && !cb_at(it); });
     auto loop = [&](cudaStream_t ls) -> int {
         for (size_t L = 0; L < sched.size(); ++L) {
             const int it = sched[L].it;
@@ -875,6 +946,7 @@ static int backward_impl(rtm_plan *p, const float *obs, const float *snap_u, con
             sp.it = (nt - 1) - it;  // backward_modeling.py:549
             sp.seq = it + 1;
             sp.snap_k = snap_of[it];
+            const int last = sched[L].two ? it + 1 : it;
             if (sched[L].two) {
                 sp.it2 = (nt - 1) - (it + 1);
                 sp.snap_k2 = snap_of[it + 1];
@@ -884,6 +956,9 @@ static int backward_impl(rtm_plan *p, const float *obs, const float *snap_u, con
                 sp.check = check_at(it);
                 CUDA_TRY((launch_mode<1>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, ls)));
             }
+            p->live = (int)((L + 1) & 1);
+            if (cb_at(last))
+                if (int rc = call_back(p, it + 1, (nt - 1) - last, ls)) return rc;
         }
         return 0;
     };
@@ -891,7 +966,12 @@ static int backward_impl(rtm_plan *p, const float *obs, const float *snap_u, con
                                            (unsigned long long)isnap, (unsigned long long)check_interval};
     for (int it = 0; it < nt; ++it)
         if (snap_of[it] >= 0) key.push_back(((unsigned long long)it << 32) | (unsigned)snap_of[it]);
-    if (int rc = run_loop(p, p->g_bwd, key, s, loop)) return rc;
+    if (p->cb) {  // host callbacks in the loop: direct launches
+        if (int rc = loop(s)) return rc;
+    } else if (int rc = run_loop(p, p->g_bwd, key, s, loop)) {
+        return rc;
+    }
+    p->live = (int)(sched.size() & 1);  // also when a replayed graph ran the loop
     p->launches += (long long)sched.size();
     const int blocks = 148 * 8;
     const size_t n = (size_t)p->g.nx * p->g.nz;
@@ -1101,6 +1181,7 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
     float *in[NFIELD] = {}, *out[NFIELD] = {};
     for (int f = 0; f < NADJ; ++f) in[f] = p->d_state[0][f];
     p->launches = 0;
+    p->live = -1;
     auto check_at = [&](int it) { return check_interval > 0 && it % check_interval == 0; };
     auto save_at = [&](int it) { return (it + 1) % ckpt_every == 0 && it + 1 < nt; };
     const std::vector<LoopLaunch> sched =
@@ -1186,6 +1267,7 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
     bs.add(seg, nslots * slot * sizeof(float));
     bs.add(gsum, (size_t)3 * NGRAD * gfl * sizeof(float));
     bs.add(gwt, (size_t)3 * nt * p->nsrc_total * sizeof(float));
+    p->live = -1;
     auto body = [&]() -> int {
         if (int r = bs.begin(s)) return r;
         CUDA_TRY(cudaMemsetAsync(p->d_flags, 0, p->nshots * sizeof(int), s));
@@ -1377,6 +1459,7 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
     bs.add(image, (size_t)3 * p->g.nx * p->g.nz * sizeof(float));
     bs.add(stack, (size_t)3 * p->g.nx * p->g.nz * sizeof(double));
     bs.add(buf, nbuf * sizeof(float));
+    p->live = -1;
     auto body = [&]() -> int {
         if (int rc = bs.begin(s)) return rc;
         if (int rc = zero_state(p, s)) return rc;

@@ -28,6 +28,35 @@ def pick_modes(psv_sources, sh_sources, regular):
     return m or PSV
 
 
+def run_with_display(plan, every, display_callback, dx, dz, run):
+    """Run ``run()`` with the plan's step callback calling
+    display_callback(u, v, w, step, nx, nz, dx, dz) with host copies of shot
+    0's live wavefield (forward: every ``every`` steps; backward: at the
+    imaging steps).  An exception in display_callback stops the time loop and
+    is re-raised."""
+    from ._lib import RtmError
+    nx, nz = plan.shots[0].nx, plan.nz
+    err = []
+
+    def cb(step):
+        try:
+            f = plan.wavefield(0).cpu().numpy()
+            display_callback(f[0], f[1], f[2], step, nx, nz, dx, dz)
+            return 0
+        except BaseException as e:  # noqa: BLE001 - re-raised after the C call returns
+            err.append(e)
+            return 1
+    plan.set_callback(every, cb)
+    try:
+        return run()
+    except RtmError:
+        if err:
+            raise err[0]
+        raise
+    finally:
+        plan.set_callback(0, None)
+
+
 class ForwardModeling:
     """Forward modeling of P-SV and SH waves (forward_modeling.py:32-79).
 
@@ -91,12 +120,7 @@ class ForwardModeling:
         1 / 2 / 3 when u / v / w became non-finite (highest code wins)."""
         if display_callback is not None:
             return self._run_with_callback(save, display_callback, stability_check_interval)
-        flags, seis, snaps, isnaps = self.plan.forward(self._wavelets, save=save, isnap=self.isnap,
-                                                       check_interval=stability_check_interval)
-        self._seis = seis
-        if save:
-            self._expose_snapshots(snaps, isnaps)
-        return int(flags[0])
+        return self._run_plain(save, stability_check_interval)
 
     def _expose_snapshots(self, snaps, isnaps):
         n = self.nt // self.isnap
@@ -113,23 +137,18 @@ class ForwardModeling:
         self._snap_plan_pitch = self.plan.pitch
 
     def _run_with_callback(self, save, display_callback, stability_check_interval):
-        """Callback path: the reference calls display_callback(u, v, w, it, nx,
-        nz, dx, dz) with host copies at it % isnap == 0 (fm:553-559).  Wavefields
-        at those steps are taken from snapshot-interval runs of the same plan."""
-        ci = stability_check_interval
-        flags, seis, snaps, isnaps = self.plan.forward(self._wavelets, save=True, isnap=self.isnap,
-                                                       check_interval=ci)
+        """Callback path: like the reference (forward_modeling.py:553-559),
+        display_callback(u, v, w, it, nx, nz, dx, dz) receives host copies of
+        the live wavefield after every step with it % isnap == 0, it = 0
+        included, during the run; no callback follows a failed finite check.
+        The time loop then runs as direct launches ending at those steps."""
+        return run_with_display(self.plan, self.isnap, display_callback, self.dx, self.dz,
+                                lambda: self._run_plain(save, stability_check_interval))
+
+    def _run_plain(self, save, stability_check_interval):
+        flags, seis, snaps, isnaps = self.plan.forward(self._wavelets, save=save, isnap=self.isnap,
+                                                       check_interval=stability_check_interval)
         self._seis = seis
-        n = self.nt // self.isnap
-        for k in range(n):
-            it = (k + 1) * self.isnap
-            if it > self.nt - 1:
-                break
-            vs = []
-            for c in range(3):
-                vs.append(np.zeros((self.nx, self.nz), np.float32) if snaps[c] is None
-                          else self.plan.snapshot_view(snaps[c], n)[:, :, k].cpu().numpy())
-            display_callback(vs[0], vs[1], vs[2], it, self.nx, self.nz, self.dx, self.dz)
         if save:
             self._expose_snapshots(snaps, isnaps)
         return int(flags[0])

@@ -148,6 +148,30 @@ class Plan:
                     _stream(stream)), "rtm_backward_normalized")
         return flags, img, stack
 
+    def set_callback(self, forward_every, fn):
+        """Host step callback (rtm_plan_set_callback): ``fn(step)`` after every
+        forward step with step % forward_every == 0 and after every backward
+        imaging step (its time t), with the live wavefield available through
+        ``wavefield``.  A non-zero return (or an exception, re-raised by the
+        caller) stops the loop.  ``fn`` None clears it."""
+        L = _lib.lib()
+        if fn is None:
+            self._cb = None
+            check(L.rtm_plan_set_callback(self.h, 0, _lib.STEP_CALLBACK(), None), "rtm_plan_set_callback")
+            return
+        self._cb = _lib.STEP_CALLBACK(lambda user, step: int(fn(int(step)) or 0))  # kept alive with the plan
+        check(L.rtm_plan_set_callback(self.h, int(forward_every), self._cb, None), "rtm_plan_set_callback")
+
+    def wavefield(self, shot=0, stream=None):
+        """(3, nx_shot, nz) float32 device copy of the live u, v, w of one
+        shot (rtm_plan_wavefield)."""
+        s = self.shots[shot]
+        out = torch.empty((3, s.nx, self.nz), dtype=torch.float32, device=self.device)
+        with torch.cuda.device(self.device):
+            check(_lib.lib().rtm_plan_wavefield(self.h, int(shot), _ptr(out[0]), _ptr(out[1]), _ptr(out[2]),
+                                                _stream(stream)), "rtm_plan_wavefield")
+        return out
+
     def _comp_active(self, c):
         return bool(self.modes & SH) if c == 1 else bool(self.modes & PSV)
 
