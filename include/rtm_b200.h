@@ -171,12 +171,14 @@ size_t rtm_plan_state_floats(const rtm_plan *plan);
 /* Checkpoint slots for interval ckpt_every: ceil(nt / ckpt_every) - 1. */
 int rtm_plan_num_checkpoints(const rtm_plan *plan, int ckpt_every);
 
-/* Checkpoint storage: FP32 (exact), or 16 bits per value with one scale per
- * block, a block being one row of one shot's field over 60 columns (30 for
- * plans with vec 1), amax = max |x| over the block:
- *   RTM_CKPT_F16 / RTM_CKPT_BF16: half / bfloat16 of x * 32752 / amax;
- *   RTM_CKPT_I16: round(x * 32767 / amax) as int16 (block floating point:
- *                 15 bits relative to the block maximum, against 11 for F16).
+/* Checkpoint storage: FP32 (exact), or 16 bits per value with one shared
+ * exponent S per block, a block being one row of one shot's field over 60
+ * columns (30 for plans with vec 1), S chosen so that the block's largest
+ * magnitude times 2^S lies in [2^14, 2^15):
+ *   RTM_CKPT_F16 / RTM_CKPT_BF16: half / bfloat16 of x * 2^S;
+ *   RTM_CKPT_I16: round(x * 2^S) as int16 (block floating point: values to
+ *                 within 2^-15 of the block maximum, against 2^-11 of each
+ *                 value for F16).
  * The compressed copy is written by the step launch that produces the
  * checkpointed state (no extra pass over the wavefield). */
 enum { RTM_CKPT_F32 = 0, RTM_CKPT_F16 = 1, RTM_CKPT_BF16 = 2, RTM_CKPT_I16 = 3 };

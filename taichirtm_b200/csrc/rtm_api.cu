@@ -1064,17 +1064,17 @@ static size_t ckpt_elem(int dtype) { return dtype == RTM_CKPT_F32 ? 4 : 2; }
 static size_t ckpt_data_bytes(const rtm_plan *p, int dtype) {
     return ((size_t)NADJ * p->state_floats * ckpt_elem(dtype) + 255) & ~size_t(255);
 }
-// Block scales of a compressed slot: one per (field, padded state row, block
-// of ckpt_block_cols(vec) columns).
+// Block exponents of a compressed slot: one int32 per (field, padded state
+// row, block of ckpt_block_cols(vec) columns).
 static int ckpt_blocks_per_row(const rtm_plan *p) { return p->nstrips * 30 * p->vec / ckpt_block_cols(p->vec); }
-static long long ckpt_scales_per_field(const rtm_plan *p) {
+static long long ckpt_shifts_per_field(const rtm_plan *p) {
     return (long long)(p->state_floats / (size_t)p->pitch) * ckpt_blocks_per_row(p);
 }
-static size_t ckpt_scale_bytes(const rtm_plan *p) {
-    return ((size_t)NADJ * (size_t)ckpt_scales_per_field(p) * sizeof(float) + 255) & ~size_t(255);
+static size_t ckpt_shift_bytes(const rtm_plan *p) {
+    return ((size_t)NADJ * (size_t)ckpt_shifts_per_field(p) * sizeof(int) + 255) & ~size_t(255);
 }
 static size_t ckpt_slot_total(const rtm_plan *p, int dtype) {
-    return ckpt_data_bytes(p, dtype) + (dtype == RTM_CKPT_F32 ? 0 : ckpt_scale_bytes(p));
+    return ckpt_data_bytes(p, dtype) + (dtype == RTM_CKPT_F32 ? 0 : ckpt_shift_bytes(p));
 }
 
 size_t rtm_plan_checkpoint_bytes(const rtm_plan *p, int ckpt_every, int ckpt_dtype) {
@@ -1085,7 +1085,7 @@ size_t rtm_plan_checkpoint_bytes(const rtm_plan *p, int ckpt_every, int ckpt_dty
 
 namespace {
 
-// Checkpoint slot c: data, then (compressed dtypes) its block-scale table.
+// Checkpoint slot c: data, then (compressed dtypes) its block-exponent table.
 unsigned char *ckpt_slot(const rtm_plan *p, void *ckpt, int dtype, int c) {
     return static_cast<unsigned char *>(ckpt) + (size_t)c * ckpt_slot_total(p, dtype);
 }
@@ -1095,9 +1095,9 @@ CkptOut ckpt_out(const rtm_plan *p, void *ckpt, int dtype, int c) {
     unsigned char *slot = ckpt_slot(p, ckpt, dtype, c);
     CkptOut o{};
     o.data = slot;
-    o.scale = reinterpret_cast<float *>(slot + ckpt_data_bytes(p, dtype));
+    o.shift = reinterpret_cast<int *>(slot + ckpt_data_bytes(p, dtype));
     o.field_elems = (long long)p->state_floats;
-    o.scale_per_field = ckpt_scales_per_field(p);
+    o.shift_per_field = ckpt_shifts_per_field(p);
     o.dtype = dtype;
     o.nblk = ckpt_blocks_per_row(p);
     return o;
@@ -1109,10 +1109,10 @@ int ckpt_load(rtm_plan *p, const void *ckpt, int dtype, int c, float *const *dst
     const CkptOut o = ckpt_out(p, const_cast<void *>(ckpt), dtype, c);
     CkptIn ci{};
     ci.data = o.data;
-    ci.scale = o.scale;
+    ci.shift = o.shift;
     for (int f = 0; f < NADJ; ++f) ci.dst[f] = dst[f];
     ci.field_elems = o.field_elems;
-    ci.scale_per_field = o.scale_per_field;
+    ci.shift_per_field = o.shift_per_field;
     ci.shots = p->d_shots;
     ci.pitch = p->pitch;
     ci.ncols = p->nstrips * 30 * p->vec;
