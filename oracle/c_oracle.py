@@ -33,13 +33,21 @@ def max_threads():
     return int(lib().rtm_oracle_max_threads_f32())
 
 
+def _comps_mask(snap_comps):
+    return sum(1 << c for c in sorted(set(snap_comps)))
+
+
 def forward(mu, lam, rho, dx, dz, nt, fs, fw, src, wu, wv, ww, rec, isnap=10, surface=None,
             save=False, check_interval=100, dtype=np.float32, modes=3, nthreads=0, nt_run=0,
-            setup_f64=True):
+            setup_f64=True, snap_comps=(0, 1, 2)):
     """ForwardModeling.run restated in C.  ``setup_f64`` evaluates the one-time
     material averages in double (see rtm_oracle.c: the reference's f32 4-point
-    harmonic mean overflows for mu > ~4.3e9 Pa).  Returns dict(flag, seis (3, nrec, nt),
-    snaps (3, nsnap, nx, nz) or None, isnaps, num_snaps)."""
+    harmonic mean overflows for mu > ~4.3e9 Pa).  ``snap_comps``: the
+    components (0 u, 1 v, 2 w) whose snapshots are kept, in that order (the
+    others image as zero in ``backward``).  Returns dict(flag, seis (3, nrec,
+    nt), snaps (len(snap_comps), nsnap, nx, nz) or None, isnaps, num_snaps,
+    snap_comps)."""
+    snap_comps = tuple(sorted(set(snap_comps)))
     sfx = "f32" if dtype == np.float32 else "f64"
     mu, lam, rho = (np.ascontiguousarray(x, dtype) for x in (mu, lam, rho))
     nx, nz = mu.shape
@@ -49,7 +57,7 @@ def forward(mu, lam, rho, dx, dz, nt, fs, fw, src, wu, wv, ww, rec, isnap=10, su
     sm = None if surface is None else np.ascontiguousarray(surface, dtype)
     seis = np.zeros((3, len(rec), nt), dtype)
     num_snaps = nt // isnap if save else 0
-    snaps = np.zeros((3, num_snaps, nx, nz), dtype) if save else None
+    snaps = np.zeros((len(snap_comps), num_snaps, nx, nz), dtype) if save else None
     isnaps = np.zeros(max(num_snaps, 1), np.int32)
     f = getattr(lib(), "rtm_oracle_forward_" + sfx)
     flag = f(ctypes.c_int(nx), ctypes.c_int(nz), ctypes.c_double(dx), ctypes.c_double(dz),
@@ -57,21 +65,27 @@ def forward(mu, lam, rho, dx, dz, nt, fs, fw, src, wu, wv, ww, rec, isnap=10, su
              _p(sm), ctypes.c_int(len(src)), _p(src), _p(wu), _p(wv), _p(ww),
              ctypes.c_int(len(rec)), _p(rec), _p(seis), ctypes.c_int(isnap), ctypes.c_int(int(save)),
              _p(snaps), _p(isnaps), ctypes.c_int(check_interval), ctypes.c_int(modes),
-             ctypes.c_int(nthreads), ctypes.c_int(nt_run), ctypes.c_int(int(setup_f64)))
-    return dict(flag=int(flag), seis=seis, snaps=snaps, isnaps=isnaps[:num_snaps], num_snaps=num_snaps)
+             ctypes.c_int(nthreads), ctypes.c_int(nt_run), ctypes.c_int(int(setup_f64)),
+             ctypes.c_int(_comps_mask(snap_comps)))
+    return dict(flag=int(flag), seis=seis, snaps=snaps, isnaps=isnaps[:num_snaps], num_snaps=num_snaps,
+                snap_comps=snap_comps)
 
 
 def backward(mu, lam, rho, dx, dz, nt, fs, fw, rec, obs, snaps, isnaps, num_snaps, isnap,
              surface=None, check_interval=100, dtype=np.float32, modes=3, nthreads=0, nt_run=0,
-             setup_f64=True):
+             setup_f64=True, snap_comps=(0, 1, 2)):
     """BackwardModeling.run_calc restated in C.  ``obs`` is (3, nrec, nt),
-    ``snaps`` (3, nsnap, nx, nz).  Returns dict(flag, img (3, nx, nz))."""
+    ``snaps`` (len(snap_comps), nsnap, nx, nz) holding the components
+    ``snap_comps`` (the forward's).  Returns dict(flag, img (3, nx, nz))."""
+    snap_comps = tuple(sorted(set(snap_comps)))
     sfx = "f32" if dtype == np.float32 else "f64"
     mu, lam, rho = (np.ascontiguousarray(x, dtype) for x in (mu, lam, rho))
     nx, nz = mu.shape
     rec = np.ascontiguousarray(np.asarray(rec).reshape(-1, 2), np.int32)
     obs = np.ascontiguousarray(obs, dtype)
     snaps = np.ascontiguousarray(snaps, dtype)
+    if snaps.shape[0] != len(snap_comps):
+        raise ValueError(f"snaps holds {snaps.shape[0]} components, snap_comps names {len(snap_comps)}")
     isnaps = np.ascontiguousarray(np.asarray(isnaps).reshape(-1), np.int32)
     if isnaps.size == 0:
         isnaps = np.zeros(1, np.int32)
@@ -83,5 +97,5 @@ def backward(mu, lam, rho, dx, dz, nt, fs, fw, rec, obs, snaps, isnaps, num_snap
              _p(sm), ctypes.c_int(len(rec)), _p(rec), _p(obs), _p(snaps), _p(isnaps),
              ctypes.c_int(num_snaps), ctypes.c_int(isnap), _p(img), ctypes.c_int(check_interval),
              ctypes.c_int(modes), ctypes.c_int(nthreads), ctypes.c_int(nt_run),
-             ctypes.c_int(int(setup_f64)))
+             ctypes.c_int(int(setup_f64)), ctypes.c_int(_comps_mask(snap_comps)))
     return dict(flag=int(flag), img=img)

@@ -294,12 +294,22 @@ static int check_finite(prop_t *p, int base) {
     return code;
 }
 
+/* Snapshot storage of component c (0 u, 1 v, 2 w) in a buffer holding only
+ * the components whose bit is set in `comps`, in order: its slab index, or
+ * -1 when c is not stored. */
+static int comp_slab(int comps, int c) {
+    if (!(comps & (1 << c))) return -1;
+    int k = 0;
+    for (int q = 0; q < c; ++q) k += (comps >> q) & 1;
+    return k;
+}
+
 int FN(rtm_oracle_forward)(int nx, int nz, double dx, double dz, int nt, double fs, int fw,
                            const REAL *mu, const REAL *lam, const REAL *rho, const REAL *surface,
                            int nsrc, const int *src, const REAL *wu, const REAL *wv, const REAL *ww,
                            int nrec, const int *rec, REAL *seis, int isnap, int save, REAL *snaps,
                            int *isnaps, int check_interval, int modes, int nthreads, int nt_run,
-                           int setup_f64) {
+                           int setup_f64, int comps) {
     if (nthreads > 0) omp_set_num_threads(nthreads);
     prop_t P, *p = &P;
     if (prop_init(p, nx, nz, dx, dz, fs, fw, mu, lam, rho, surface, setup_f64)) return -1;
@@ -331,9 +341,11 @@ int FN(rtm_oracle_forward)(int nx, int nz, double dx, double dz, int nt, double 
         }
         if (save && it % isnap == 0 && it != 0) { /* forward_modeling.py:569-572 */
             int k = it / isnap - 1;
-            memcpy(snaps + ((size_t)0 * num_snaps + k) * n, p->u, n * sizeof(REAL));
-            memcpy(snaps + ((size_t)1 * num_snaps + k) * n, p->v, n * sizeof(REAL));
-            memcpy(snaps + ((size_t)2 * num_snaps + k) * n, p->w, n * sizeof(REAL));
+            const REAL *src3[3] = {p->u, p->v, p->w};
+            for (int c = 0; c < 3; ++c) {
+                const int sl = comp_slab(comps, c);
+                if (sl >= 0) memcpy(snaps + ((size_t)sl * num_snaps + k) * n, src3[c], n * sizeof(REAL));
+            }
             isnaps[k] = it;
         }
     }
@@ -346,7 +358,7 @@ int FN(rtm_oracle_backward)(int nx, int nz, double dx, double dz, int nt, double
                             int nrec, const int *rec, const REAL *obs, const REAL *snaps,
                             const int *isnaps, int num_snaps, int isnap, REAL *img,
                             int check_interval, int modes, int nthreads, int nt_run,
-                            int setup_f64) {
+                            int setup_f64, int comps) {
     if (nthreads > 0) omp_set_num_threads(nthreads);
     prop_t P, *p = &P;
     if (prop_init(p, nx, nz, dx, dz, fs, fw, mu, lam, rho, surface, setup_f64)) return -1;
@@ -368,14 +380,15 @@ int FN(rtm_oracle_backward)(int nx, int nz, double dx, double dz, int nt, double
         if (t > 0 && t % isnap == 0) { /* backward_modeling.py:556-564 */
             int k = t / isnap - 1;
             if (k >= 0 && k < num_snaps && isnaps[k] == t) {
-                const REAL *su = snaps + ((size_t)0 * num_snaps + k) * n;
-                const REAL *sv = snaps + ((size_t)1 * num_snaps + k) * n;
-                const REAL *sw = snaps + ((size_t)2 * num_snaps + k) * n;
+                const REAL *bw3[3] = {p->u, p->v, p->w};
+                for (int c = 0; c < 3; ++c) {  /* components not stored image as zero */
+                    const int sl = comp_slab(comps, c);
+                    if (sl < 0) continue;
+                    const REAL *sn = snaps + ((size_t)sl * num_snaps + k) * n;
+                    const REAL *b = bw3[c];
+                    REAL *im = img + (size_t)c * n;
 #pragma omp parallel for
-                for (size_t q = 0; q < n; ++q) {
-                    img[q] += su[q] * p->u[q];
-                    img[n + q] += sv[q] * p->v[q];
-                    img[2 * n + q] += sw[q] * p->w[q];
+                    for (size_t q = 0; q < n; ++q) im[q] += sn[q] * b[q];
                 }
             }
         }

@@ -131,3 +131,25 @@ def test_imaging_slots_and_source_normalization_definition():
     ill = (snaps[0][..., [0, 2, 5]] ** 2).sum(-1)
     assert np.allclose(out[0], img[0] / (ill + 0.1 * ill.max()))
     assert np.all(out[1] == 0.0)
+
+
+def test_c_oracle_snapshot_components_subset_images_the_same():
+    """Keeping only the imaged components' snapshots (snap_comps) gives the
+    same image for those components and zero for the others."""
+    from oracle import c_oracle
+    from taichirtm_b200 import synthetic as S
+    s = S.config1(nt=120)
+    sh = s.shots[0]
+    mu, lam, rho = s.material()
+    kw = dict(dx=s.dx, dz=s.dz, nt=s.nt, fs=s.fs, fw=s.fw, dtype=np.float64, modes=1)
+    wv = dict(wu=sh.wavelets[0], wv=sh.wavelets[1], ww=sh.wavelets[2])
+    f3 = c_oracle.forward(mu, lam, rho, src=sh.src, rec=sh.rec, save=True, isnap=3, **wv, **kw)
+    f2 = c_oracle.forward(mu, lam, rho, src=sh.src, rec=sh.rec, save=True, isnap=3, snap_comps=(0, 2), **wv, **kw)
+    assert f2["snaps"].shape[0] == 2
+    obs = 0.5 * f3["seis"]
+    b3 = c_oracle.backward(mu, lam, rho, rec=sh.rec, obs=obs, snaps=f3["snaps"], isnaps=f3["isnaps"],
+                           num_snaps=f3["num_snaps"], isnap=3, **kw)
+    b2 = c_oracle.backward(mu, lam, rho, rec=sh.rec, obs=obs, snaps=f2["snaps"], isnaps=f2["isnaps"],
+                           num_snaps=f2["num_snaps"], isnap=3, snap_comps=(0, 2), **kw)
+    assert np.array_equal(b3["img"][[0, 2]], b2["img"][[0, 2]])
+    assert np.abs(b2["img"][1]).max() == 0.0
