@@ -156,6 +156,60 @@ def reference_arm(args, rank):
     return 0
 
 
+# ------------------------------------------------------------ large model (c5)
+def c5_host_legs(line):
+    """Host legs of the large-model line, on its shot 0 (a 1339 x 1601 window):
+    the cpu_baseline (the C restatement in FP32, both P-SV and SH as the
+    reference runs, a bounded sample of the time axis scaled to one shot),
+    and, as the checker, the FP64 run of the same restatement against which
+    the shot's RTM image is compared for snapshots and each checkpoint
+    storage (full length; snapshots and imaging every 160 steps to bound the
+    host memory of the FP64 snapshots)."""
+    import torch
+    from oracle import c_oracle
+    from taichirtm_b200.batch import BatchedRTM
+    from taichirtm_b200.plan import ShotGeometry
+    sv, K, tune = line["_survey"], line["_K"], line["_tune"]
+    sh = sv.shots[0]
+    crop = [np.ascontiguousarray(x[sh.x0:sh.x0 + sh.nx]) for x in sv.material(migration=True)]
+    nthreads = os.cpu_count() or 1
+    n_run = 400
+    kw = dict(dx=sv.dx, dz=sv.dz, nt=sv.nt, fs=sv.fs, fw=sv.fw, nthreads=nthreads)
+    t0 = time.perf_counter()
+    f = c_oracle.forward(*crop, src=sh.src, wu=sh.wavelets[0], wv=sh.wavelets[1], ww=sh.wavelets[2], rec=sh.rec,
+                         nt_run=n_run, save=True, isnap=ISNAP, dtype=np.float32, modes=3, **kw)
+    c_oracle.backward(*crop, rec=sh.rec, obs=np.zeros((3, len(sh.rec), sv.nt), np.float32), snaps=f["snaps"],
+                      isnaps=np.arange(1, sv.nt // ISNAP + 1) * ISNAP, num_snaps=sv.nt // ISNAP, isnap=ISNAP,
+                      nt_run=n_run, dtype=np.float32, modes=3, **kw)
+    sec = (time.perf_counter() - t0) * sv.nt / n_run
+    del f
+    line["cpu_baseline"] = dict(value=round(1.0 / sec, 5), unit="shots/s (RTM)", cores=nthreads, kind="port",
+                                sample=f"shot 0 ({sh.nx}x{sv.nz} window), {n_run} of {sv.nt} steps of both phases, "
+                                       f"FP32, P-SV+SH as the reference runs, scaled x{sv.nt // n_run} to one shot")
+    ie = 160
+    f64 = c_oracle.forward(*crop, src=sh.src, wu=sh.wavelets[0], wv=sh.wavelets[1], ww=sh.wavelets[2], rec=sh.rec,
+                           save=True, isnap=ie, snap_comps=(0, 2), dtype=np.float64, modes=1, **kw)
+    obs = (0.5 * f64["seis"]).astype(np.float32)
+    img64 = c_oracle.backward(*crop, rec=sh.rec, obs=obs, snaps=f64["snaps"], isnaps=f64["isnaps"],
+                              num_snaps=f64["num_snaps"], isnap=ie, snap_comps=(0, 2), dtype=np.float64, modes=1,
+                              **kw)["img"]
+    del f64
+    r = BatchedRTM(*sv.material(migration=True), sv.dx, sv.dz, sv.fs, sv.nt, sv.fw,
+                   [ShotGeometry(sh.x0, sh.nx, sh.src, sh.rec)], tune=tune, graphs=False)
+    errs = {}
+    for dt in (None, "f32", "f16", "i16"):
+        ck = dict(every=K, dtype=dt) if dt else None
+        _, _, st = r.migrate(sh.wavelets, obs, isnap=ie, checkpoint=ck)
+        img = st.cpu().numpy()[:, sh.x0:sh.x0 + sh.nx]
+        a, b = img[[0, 2]].astype(np.float64), img64[[0, 2]]
+        errs[f"image_{dt or 'snapshots'}_vs_fp64_rel_l2"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    r.close()
+    torch.cuda.synchronize()
+    line["errors_vs_fp64"] = dict(errs, case=f"shot 0 ({sh.nx}x{sv.nz} window), all {sv.nt} steps, imaging every "
+                                             f"{ie} steps, observed data = half the FP64 seismograms; "
+                                             "the FP64 C restatement as the checker")
+
+
 # ------------------------------------------------------------- plain one-shot RTM
 def plain_single_shot(args, rank):
     """Plain single-shot RTM (forward with snapshots at the reference's
@@ -284,6 +338,17 @@ def main():
         return reference_arm(args, rank)
     if args.workload in ("c1", "c2"):
         return plain_single_shot(args, rank)
+    if args.workload == "c5":
+        from taichirtm_b200 import benchmarks
+        import torch
+        torch.cuda.set_device(local)
+        line = benchmarks.run_c5(args)
+        if not args.no_cpu:
+            c5_host_legs(line)
+        for k in [k for k in line if k.startswith("_")]:
+            line.pop(k)
+        print(json.dumps(line), flush=True)
+        return 0
     if args.workload != "c3":
         from taichirtm_b200 import benchmarks
         return benchmarks.run(args)
