@@ -139,7 +139,7 @@ def test_large_model_checkpointed_rtm_and_gradient_vs_fp64():
     # FP64: forward with snapshots and backward with imaging per shot, the
     # observed data being half the migration model's own FP64 seismograms
     img64 = np.zeros((3, sv.nx, sv.nz))
-    obs_parts = []
+    obs_parts, seis64 = [], []
     for s in sub:
         crop = [np.ascontiguousarray(x[s.x0:s.x0 + s.nx]) for x in (mu, lam, rho)]
         kw = dict(dx=sv.dx, dz=sv.dz, nt=sv.nt, fs=sv.fs, fw=sv.fw, dtype=np.float64, modes=1)
@@ -150,12 +150,15 @@ def test_large_model_checkpointed_rtm_and_gradient_vs_fp64():
                               num_snaps=f["num_snaps"], isnap=16, snap_comps=(0, 2), **kw)
         img64[:, s.x0:s.x0 + s.nx] += b["img"]
         obs_parts.append(o)
+        seis64.append(f["seis"])
         del f
     obs = np.concatenate(obs_parts, axis=1)
     wav = np.concatenate([s.wavelets for s in sub], axis=1)
     mu32, lam32, rho32 = sv.material(migration=True)
     tune = dict(vec=2, rows=32, warps=1, tsteps=2, prefetch=3)
     rtm = BatchedRTM(mu32, lam32, rho32, sv.dx, sv.dz, sv.fs, sv.nt, sv.fw, geo, tune=tune, graphs=False)
+    _, seis, _, _ = rtm.forward(wav)
+    seis_err = rel_l2(seis.cpu().numpy()[[0, 2]], np.concatenate(seis64, axis=1)[[0, 2]])
     img_err = {}
     for dt in ("f32", "f16", "i16"):
         ff, fb, st = rtm.migrate(wav, obs, isnap=16, checkpoint=dict(every=K, dtype=dt))
@@ -175,10 +178,11 @@ def test_large_model_checkpointed_rtm_and_gradient_vs_fp64():
     dirs = _directions(sv.vp.shape, [np.mean(x) for x in m0], rng, 3)
     grad_err = _fd_check(sv, sub, m0, obs.astype(np.float64), grads, dirs)
     flat = {k: np.concatenate([g.ravel() for g in v]) for k, v in grads.items()}
-    print("large model vs FP64: image", {k: f"{v:.2e}" for k, v in img_err.items()},
+    print(f"large model vs FP64: seismograms {seis_err:.2e}, image", {k: f"{v:.2e}" for k, v in img_err.items()},
           "gradient directional", {k: f"{max(v):.2e}" for k, v in grad_err.items()},
           "gradient rel-L2 vs FP32 checkpoints: f16 %.2e i16 %.2e" % (rel_l2(flat["f16"], flat["f32"]),
                                                                        rel_l2(flat["i16"], flat["f32"])))
+    assert seis_err <= SEIS_TOL, seis_err
     assert img_err["f32"] <= IMG_TOL and img_err["i16"] <= IMG_TOL, img_err
     assert max(grad_err["f32"]) <= GRAD_TOL and max(grad_err["i16"]) <= GRAD_TOL, grad_err
     assert img_err["f16"] <= 1e-3, img_err  # reported; FP16 keeps 11 bits per value
@@ -203,7 +207,12 @@ def test_config4_gradient_full_size_vs_fp64_finite_differences():
     m = [torch.tensor(x, dtype=torch.float64, device="cuda", requires_grad=True) for x in m0]
     l2_misfit(m[0], m[1], m[2], prob, torch.as_tensor(obs)).backward()
     g = [x.grad.cpu().numpy() for x in m]
+    mu0, lam0, rho0 = (torch.as_tensor(x.astype(np.float32)) for x in _lame64(*m0))
+    d, _, _ = prob.forward(lam0, mu0, rho0)
+    seis_err = rel_l2(d.cpu().numpy()[[0, 2]], _fp64_seis(sv, sub, *m0)[[0, 2]])
     prob.close()
+    print(f"config 4 seismograms at the starting model vs FP64: {seis_err:.2e}")
+    assert seis_err <= SEIS_TOL, seis_err
     rng = np.random.default_rng(104)
     dirs = _directions(sv.vp.shape, [np.mean(x) for x in m0], rng, 3)
     errs = _fd_check(sv, sub, m0, obs.astype(np.float64), {"f32": g}, dirs)["f32"]

@@ -120,6 +120,7 @@ def test_config1_psv_rtm_vs_fp64_oracle():
     assert bw.run_calc(fm.u_save_field, fm.v_save_field, fm.w_save_field, fm.isnaps_field, fm.num_snaps, 1) == 0
     img = np.stack(bw.get_results())
     e_img = rel_l2(img[[0, 2]], ref_img[[0, 2]])
+    print(f"config 1 P-SV RTM vs FP64: seismograms {e_seis:.2e}, image {e_img:.2e}")
     assert e_img <= IMG_TOL, e_img
     assert np.abs(img[1]).max() == 0
 
