@@ -77,8 +77,9 @@ typedef struct {
     int prefetch;   /* 1: software-pipelined row loads; 3: cp.async pipeline, rows 3 ahead in a
                        per-warp shared-memory ring (with tsteps 2: the material and 1/rho rows
                        through a 4-row ring, the state in registers); 2: row loads plus L2 cache
-                       policies (state evict-first, material evict-last); 0: plain; other values =
-                       default (1) */
+                       policies (state evict-first, material evict-last); 4: as 3 with tsteps 2, one
+                       warp per CTA and the task taken from the block index (warps is set to 1);
+                       0: plain; other values = default (1) */
     int graphs;     /* 1: capture each time loop as a CUDA graph on first use and replay it
                        while its pointers and schedule stay the same; 0 = direct launches */
     int tsteps;     /* time steps per launch of rtm_forward, rtm_backward and the

@@ -312,7 +312,7 @@ cudaError_t launch_mode(const StepParams &sp, int modes, int vec, int warps, cud
     }
 }
 
-template <int DIR, int MODE, int VEC, bool RING, bool STOREA = false, bool CKPT = false>
+template <int DIR, int MODE, int VEC, bool RING, bool STOREA = false, bool CKPT = false, bool UNI = false>
 cudaError_t launch_step2(const StepParams &sp, int warps, cudaStream_t s) {
     size_t smem = 0;
     if constexpr (RING) {
@@ -322,13 +322,13 @@ cudaError_t launch_step2(const StepParams &sp, int warps, cudaStream_t s) {
         static bool attr_set = false;  // per instantiation; raises the 48 KB default
         if (!attr_set) {
             const size_t want = std::min<size_t>(8 * ring2_smem_per_warp<MODE, VEC>(), kMaxSmem);
-            cudaError_t e = cudaFuncSetAttribute(step2_kernel<DIR, MODE, VEC, RING, STOREA, CKPT>,
+            cudaError_t e = cudaFuncSetAttribute(step2_kernel<DIR, MODE, VEC, RING, STOREA, CKPT, UNI>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
             if (e != cudaSuccess) return e;
             attr_set = true;
         }
     }
-    step2_kernel<DIR, MODE, VEC, RING, STOREA, CKPT><<<(sp.n_work + warps - 1) / warps, 32 * warps, smem, s>>>(sp);
+    step2_kernel<DIR, MODE, VEC, RING, STOREA, CKPT, UNI><<<(sp.n_work + warps - 1) / warps, 32 * warps, smem, s>>>(sp);
     return cudaGetLastError();
 }
 
@@ -366,7 +366,7 @@ cudaError_t launch_pf_ckpt(const StepParams &sp, int pfm, int warps, cudaStream_
 }
 cudaError_t launch_ckpt(const StepParams &sp, bool two, int vec, int prefetch, int warps, cudaStream_t s) {
     if (two) {
-        const bool ring = prefetch == 3;
+        const bool ring = prefetch >= 3;
         if (vec == 2)
             return ring ? launch_step2<0, RTM_PSV, 2, true, false, true>(sp, warps, s)
                         : launch_step2<0, RTM_PSV, 2, false, false, true>(sp, warps, s);
@@ -380,8 +380,15 @@ cudaError_t launch_ckpt(const StepParams &sp, bool two, int vec, int prefetch, i
     }
 }
 
+// uni (prefetch 4): the ring kernel with the task taken from blockIdx.x,
+// one warp per CTA (the plan forces warps = 1).
 template <int DIR, int MODE>
-cudaError_t launch_vec2(const StepParams &sp, int vec, bool ring, int warps, cudaStream_t s) {
+cudaError_t launch_vec2(const StepParams &sp, int vec, bool ring, bool uni, int warps, cudaStream_t s) {
+    if (uni) {
+        if (warps != 1) return cudaErrorInvalidConfiguration;
+        return vec == 2 ? launch_step2<DIR, MODE, 2, true, false, false, true>(sp, 1, s)
+                        : launch_step2<DIR, MODE, 4, true, false, false, true>(sp, 1, s);
+    }
     if (vec == 2) return ring ? launch_step2<DIR, MODE, 2, true>(sp, warps, s) : launch_step2<DIR, MODE, 2, false>(sp, warps, s);
     return ring ? launch_step2<DIR, MODE, 4, true>(sp, warps, s) : launch_step2<DIR, MODE, 4, false>(sp, warps, s);
 }
@@ -389,7 +396,7 @@ cudaError_t launch_vec2(const StepParams &sp, int vec, bool ring, int warps, cud
 // Forward recompute of the adjoint, P-SV: steps sp.it and sp.it2 in one
 // launch, storing the state after each (sp.souta, sp.sout).
 cudaError_t launch_recompute2(const StepParams &sp, int vec, int prefetch, int warps, cudaStream_t s) {
-    const bool ring = prefetch == 3;
+    const bool ring = prefetch >= 3;
     if (vec == 2)
         return ring ? launch_step2<0, RTM_PSV, 2, true, true>(sp, warps, s) : launch_step2<0, RTM_PSV, 2, false, true>(sp, warps, s);
     return ring ? launch_step2<0, RTM_PSV, 4, true, true>(sp, warps, s) : launch_step2<0, RTM_PSV, 4, false, true>(sp, warps, s);
@@ -399,11 +406,11 @@ cudaError_t launch_recompute2(const StepParams &sp, int vec, int prefetch, int w
 // creation); prefetch 3 selects the shared-memory material ring.
 template <int DIR>
 cudaError_t launch_mode2(const StepParams &sp, int modes, int vec, int prefetch, int warps, cudaStream_t s) {
-    const bool ring = prefetch == 3;
+    const bool ring = prefetch >= 3, uni = prefetch == 4;
     switch (modes) {
-        case RTM_PSV: return launch_vec2<DIR, RTM_PSV>(sp, vec, ring, warps, s);
-        case RTM_SH: return launch_vec2<DIR, RTM_SH>(sp, vec, ring, warps, s);
-        default: return launch_vec2<DIR, RTM_BOTH>(sp, vec, ring, warps, s);
+        case RTM_PSV: return launch_vec2<DIR, RTM_PSV>(sp, vec, ring, uni, warps, s);
+        case RTM_SH: return launch_vec2<DIR, RTM_SH>(sp, vec, ring, uni, warps, s);
+        default: return launch_vec2<DIR, RTM_BOTH>(sp, vec, ring, uni, warps, s);
     }
 }
 
@@ -530,7 +537,8 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
         if (tune->vec == 1 || tune->vec == 2 || tune->vec == 4) p->vec = tune->vec;
         if (tune->rows > 0) p->rows = tune->rows;
         if (tune->warps > 0 && tune->warps <= 8) p->warps = tune->warps;
-        if (tune->prefetch >= 0 && tune->prefetch <= 3) p->prefetch = tune->prefetch;
+        if (tune->prefetch >= 0 && tune->prefetch <= 4) p->prefetch = tune->prefetch;
+        if (p->prefetch == 4) p->warps = 1;  // the uniform-task kernel runs one warp per CTA
         p->use_graphs = tune->graphs == 1;
         if (tune->tsteps == 2) {
             if (p->vec == 1) {
@@ -837,7 +845,7 @@ int rtm_forward(rtm_plan *p, const float *wavelets, float *seis, int save, int i
                 CUDA_TRY((launch_mode2<0>(sp, p->g.modes, p->vec, p->prefetch, p->warps, ls)));
             } else {
                 sp.check = check_at(it);
-                CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, ls)));
+                CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (std::min(p->prefetch, 3) << 8), p->warps, ls)));
             }
             p->live = (int)((L + 1) & 1);
             if (cb_at(last))
@@ -954,7 +962,7 @@ static int backward_impl(rtm_plan *p, const float *obs, const float *snap_u, con
                 CUDA_TRY((launch_mode2<1>(sp, p->g.modes, p->vec, p->prefetch, p->warps, ls)));
             } else {
                 sp.check = check_at(it);
-                CUDA_TRY((launch_mode<1>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, ls)));
+                CUDA_TRY((launch_mode<1>(sp, p->g.modes, p->vec | (std::min(p->prefetch, 3) << 8), p->warps, ls)));
             }
             p->live = (int)((L + 1) & 1);
             if (cb_at(last))
@@ -1213,7 +1221,7 @@ int rtm_forward_checkpointed(rtm_plan *p, const float *wavelets, float *seis, in
         } else if (ln.two) {
             CUDA_TRY((launch_mode2<0>(sp, p->g.modes, p->vec, p->prefetch, p->warps, s)));
         } else {
-            CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (p->prefetch << 8), p->warps, s)));
+            CUDA_TRY((launch_mode<0>(sp, p->g.modes, p->vec | (std::min(p->prefetch, 3) << 8), p->warps, s)));
         }
         ++p->launches;
         for (int f = 0; f < NADJ; ++f) in[f] = out[f];
@@ -1361,7 +1369,7 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
                     CUDA_TRY(launch_recompute2(sp, p->vec, p->prefetch, warps, s));
                     it += 2;
                 } else {
-                    CUDA_TRY((launch_mode<0>(sp, RTM_PSV, p->vec | (p->prefetch << 8), warps, s)));
+                    CUDA_TRY((launch_mode<0>(sp, RTM_PSV, p->vec | (std::min(p->prefetch, 3) << 8), warps, s)));
                     it += 1;
                 }
                 ++p->launches;
@@ -1528,7 +1536,7 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
                     fp.snap_k2 = slot_at(it + 1);
                     CUDA_TRY((launch_mode2<0>(fp, RTM_PSV, p->vec, p->prefetch, p->warps, s)));
                 } else {
-                    CUDA_TRY((launch_mode<0>(fp, RTM_PSV, p->vec | (p->prefetch << 8), p->warps, s)));
+                    CUDA_TRY((launch_mode<0>(fp, RTM_PSV, p->vec | (std::min(p->prefetch, 3) << 8), p->warps, s)));
                 }
                 ++p->launches;
             }
@@ -1551,7 +1559,7 @@ int rtm_backward_checkpointed(rtm_plan *p, const float *wavelets, const float *o
                     CUDA_TRY((launch_mode2<1>(bp, RTM_PSV, p->vec, p->prefetch, p->warps, s)));
                 } else {
                     bp.check = check_at(it);
-                    CUDA_TRY((launch_mode<1>(bp, RTM_PSV, p->vec | (p->prefetch << 8), p->warps, s)));
+                    CUDA_TRY((launch_mode<1>(bp, RTM_PSV, p->vec | (std::min(p->prefetch, 3) << 8), p->warps, s)));
                 }
                 ++p->launches;
                 ++nb;

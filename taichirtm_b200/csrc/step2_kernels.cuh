@@ -99,8 +99,13 @@ __host__ __device__ constexpr size_t ring2_smem_per_warp() {
 // forward recompute of the FWI adjoint, which needs the state after every step.
 // CKPT: step B's state is also stored, block-scaled to 16 bits, into the
 // checkpoint slot p.ck (ckpt_pack.cuh); forward P-SV only.
-template <int DIR, int MODE, int VEC, bool RING = false, bool STOREA = false, bool CKPT = false>
-__global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
+// UNI: launched with one warp per CTA, the task is blockIdx.x.  Everything
+// derived from the task (shot, strip, row range, loop bounds, fast-path
+// choices) is then provably the same for the whole warp, so the compiler
+// keeps it in uniform registers and branches on it without divergence
+// bookkeeping; the arithmetic of every cell is unchanged.
+template <int DIR, int MODE, int VEC, bool RING = false, bool STOREA = false, bool CKPT = false, bool UNI = false>
+__global__ void __launch_bounds__(UNI ? 32 : 256) step2_kernel(const StepParams p) {
     static_assert(VEC >= 2, "two steps per launch need two halo columns per side");
     static_assert(!STOREA || DIR == 0, "only the forward recompute stores step A");
     static_assert(!CKPT || (DIR == 0 && MODE == 1), "checkpoint stores are forward P-SV");
@@ -111,7 +116,7 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     using Vel = VelRow<VEC>;
     using Mat = MatRow<VEC>;
     const int lane = threadIdx.x & 31;
-    const int task = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int task = UNI ? (int)blockIdx.x : (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (task >= p.n_work) return;
     const int4 wk = p.work[task];
     if (shot_stopped(p, wk.x)) return;
@@ -169,11 +174,11 @@ __global__ void __launch_bounds__(256) step2_kernel(const StepParams p) {
     constexpr int RF_MYX = PSV ? 5 : 0, RF_MYZ = RF_MYX + 1, RF_IR = RF_MYX + 2;
     constexpr int RF_SM = NRF - 1;
     extern __shared__ float step2_smem[];
-    float *ring = step2_smem + (size_t)(threadIdx.x >> 5) * (RING2_ROWS * NRF * 32 * VEC);
-    auto rslot = [&](int row, int f) {
-        const int s = (row + 4 * RING2_ROWS) % RING2_ROWS;  // rows >= -2
-        return ring + ((size_t)(s * NRF + f) * 32 + lane) * VEC;
-    };
+    static_assert((RING2_ROWS & (RING2_ROWS - 1)) == 0, "the ring slot is the row modulo a power of two");
+    // this lane's VEC floats of slot 0, field 0; a (slot, field) is a fixed
+    // 32-bit offset from it (rows >= -2: row & (RING2_ROWS - 1) is the slot)
+    float *const ring = step2_smem + (UNI ? 0 : (int)(threadIdx.x >> 5) * (RING2_ROWS * NRF * 32 * VEC)) + lane * VEC;
+    auto rslot = [&](int row, int f) { return ring + ((row & (RING2_ROWS - 1)) * NRF + f) * (32 * VEC); };
     auto ring_issue = [&](int row) {
         auto put = [&](int f, const float *src) {
             cp_async_vec<VEC>(rslot(row, f), src + moff + (long long)(rowc(row) + 1) * P);

@@ -89,7 +89,8 @@ def _same(a, b):
 @pytest.mark.parametrize("tune", [dict(vec=2, rows=7, warps=3), dict(vec=4, rows=16, warps=2),
                                   dict(vec=2, rows=1, warps=4), dict(vec=4, rows=2, warps=1),
                                   dict(vec=2, rows=5, warps=2, prefetch=3), dict(vec=4, rows=3, warps=1, prefetch=3),
-                                  dict(vec=2, rows=1, warps=8, prefetch=3)])
+                                  dict(vec=2, rows=1, warps=8, prefetch=3), dict(vec=2, rows=5, warps=1, prefetch=4),
+                                  dict(vec=4, rows=3, warps=1, prefetch=4)])
 def test_two_steps_per_launch_bit_identical(modes, tune):
     C = _case()
     one = _run(C, modes, dict(tune, tsteps=1), isnap=3)
@@ -99,7 +100,7 @@ def test_two_steps_per_launch_bit_identical(modes, tune):
     assert two["launches"] < one["launches"]
 
 
-@pytest.mark.parametrize("prefetch", [1, 3])
+@pytest.mark.parametrize("prefetch", [1, 3, 4])
 @pytest.mark.parametrize("isnap", [1, 2])
 def test_two_steps_imaging_every_step_and_topography(isnap, prefetch):
     C = _case(nx=90, nz=130, nt=40, fw=12, seed=5)
@@ -204,7 +205,8 @@ def test_failing_check_step_is_complete_for_every_launch_shape():
     outs = []
     for tune in (dict(vec=2, rows=4, warps=2, tsteps=1), dict(vec=2, rows=4, warps=2, tsteps=2),
                  dict(vec=1, rows=3, warps=1, prefetch=0), dict(vec=4, rows=64, warps=8, prefetch=3),
-                 dict(vec=4, rows=2, warps=8, tsteps=2), dict(vec=2, rows=6, warps=2, tsteps=2, prefetch=3)):
+                 dict(vec=4, rows=2, warps=8, tsteps=2), dict(vec=2, rows=6, warps=2, tsteps=2, prefetch=3),
+                 dict(vec=2, rows=6, warps=1, tsteps=2, prefetch=4)):
         p = Plan(C["nx"], C["nz"], C["dx"], C["dz"], C["nt"], C["fs"], C["fw"], 1,
                  [ShotGeometry(0, C["nx"], src, C["rec"])], tune=tune)
         p.set_model(mu, lam, rho)
