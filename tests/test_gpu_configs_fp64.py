@@ -191,9 +191,20 @@ def test_large_model_checkpointed_rtm_and_gradient_vs_fp64():
 def test_config4_gradient_full_size_vs_fp64_finite_differences():
     """The 1201 x 401 FWI gradient at nt 3000 with sqrt(nt) FP32 checkpoints
     (two of the eight shots: the gradient is a sum over shots), observed data
-    from the true model; 3 seeded directions."""
+    from the true model, against centred FP64 differences of J on 3 seeded
+    directions and along the gradient itself.
+
+    Two gradients are compared.  The adjoint driven by the FP64 residual
+    d64(m0) - d_obs (rounded once to FP32) isolates the discrete adjoint and
+    its FP32 arithmetic: within 1e-4 in every direction.  The end-to-end
+    gradient of l2_misfit uses the FP32 forward's own residual; the smoothed
+    starting model leaves a residual much smaller than the data, so the FP32
+    seismogram error (relative to the data) grows by ||d|| / ||r|| relative
+    to the residual, and the gradient is linear in the residual.  Its errors
+    are held to 1e-4 along the gradient and, in the random directions, to
+    that amplified FP32 floor (both printed)."""
     from taichirtm_b200 import synthetic as S
-    from taichirtm_b200.fwi import FWIProblem, l2_misfit
+    from taichirtm_b200.fwi import FWIProblem, chain_to_lame_rho, l2_misfit
     from taichirtm_b200.plan import ShotGeometry
     sv = S.config4()
     sub = [sv.shots[1], sv.shots[5]]
@@ -201,20 +212,39 @@ def test_config4_gradient_full_size_vs_fp64_finite_differences():
     wav = np.concatenate([s.wavelets for s in sub], axis=1)
     obs = _fp64_seis(sv, sub, sv.vp, sv.vs, sv.rho).astype(np.float32)
     m0 = [sv.vp_mig, sv.vs_mig, sv.rho_mig]
+    d64 = _fp64_seis(sv, sub, *m0)
     K = round(math.sqrt(sv.nt))
     prob = FWIProblem(sv.nx, sv.nz, sv.dx, sv.dz, sv.fs, sv.nt, sv.fw, geo, wav, ckpt_every=K,
                       tune=dict(vec=2, rows=16, warps=2, tsteps=2))
     m = [torch.tensor(x, dtype=torch.float64, device="cuda", requires_grad=True) for x in m0]
     l2_misfit(m[0], m[1], m[2], prob, torch.as_tensor(obs)).backward()
-    g = [x.grad.cpu().numpy() for x in m]
+    g_e2e = [x.grad.cpu().numpy() for x in m]
+    # the adjoint driven by the FP64 residual, mapped to (vp, vs, rho) like the
+    # autograd function does (fwi.py: chain_to_lame_rho, then mu = rho vs^2,
+    # lam = rho vp^2 - 2 mu)
     mu0, lam0, rho0 = (torch.as_tensor(x.astype(np.float32)) for x in _lame64(*m0))
-    d, _, _ = prob.forward(lam0, mu0, rho0)
-    seis_err = rel_l2(d.cpu().numpy()[[0, 2]], _fp64_seis(sv, sub, *m0)[[0, 2]])
+    d, ck, _ = prob.forward(lam0, mu0, rho0)
+    seis_err = rel_l2(d.cpu().numpy()[[0, 2]], d64[[0, 2]])
+    r64 = d64 - obs.astype(np.float64)
+    r64[1] = 0.0
+    gcoef, _ = prob.adjoint(torch.as_tensor(r64.astype(np.float32)), ck)
     prob.close()
-    print(f"config 4 seismograms at the starting model vs FP64: {seis_err:.2e}")
-    assert seis_err <= SEIS_TOL, seis_err
+    vp, vs, rho = (torch.tensor(x, dtype=torch.float64, device="cuda", requires_grad=True) for x in m0)
+    mu_t = rho * vs * vs
+    lam_t = rho * vp * vp - 2.0 * mu_t
+    g_lam, g_mu, g_rho = chain_to_lame_rho(gcoef, mu_t.detach(), rho.detach())
+    torch.autograd.backward([lam_t, mu_t, rho], [g_lam, g_mu, g_rho])
+    g_adj = [vp.grad.cpu().numpy(), vs.grad.cpu().numpy(), rho.grad.cpu().numpy()]
+    kappa = float(np.linalg.norm(d64[[0, 2]]) / np.linalg.norm(r64[[0, 2]]))
     rng = np.random.default_rng(104)
     dirs = _directions(sv.vp.shape, [np.mean(x) for x in m0], rng, 3)
-    errs = _fd_check(sv, sub, m0, obs.astype(np.float64), {"f32": g}, dirs)["f32"]
-    print("config 4 gradient vs FP64 finite differences:", [f"{e:.2e}" for e in errs])
-    assert max(errs) <= GRAD_TOL, errs
+    dirs.append([gi / np.abs(gi).max() * np.mean(pi) for gi, pi in zip(g_adj, m0)])  # along the gradient
+    errs = _fd_check(sv, sub, m0, obs.astype(np.float64), {"adjoint": g_adj, "end_to_end": g_e2e}, dirs)
+    floor = seis_err * kappa
+    print(f"config 4 vs FP64: seismograms {seis_err:.2e}; ||d||/||r|| {kappa:.1f} (FP32 floor relative to the "
+          f"residual {floor:.1e}); directional errors (3 random, along the gradient): adjoint "
+          f"{[f'{e:.2e}' for e in errs['adjoint']]}, end to end {[f'{e:.2e}' for e in errs['end_to_end']]}")
+    assert seis_err <= SEIS_TOL, seis_err
+    assert max(errs["adjoint"]) <= GRAD_TOL, errs
+    assert errs["end_to_end"][-1] <= GRAD_TOL, errs
+    assert max(errs["end_to_end"]) <= max(GRAD_TOL, 2.0 * floor), (errs, floor)
