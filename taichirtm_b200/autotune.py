@@ -124,7 +124,10 @@ def best_shape(make_plan, nz, shots, modes, nt, candidates=None, refresh=False):
 # warp tasks than the forward step, so FWIProblem(tune="auto") times the
 # gradient itself (checkpointed forward + adjoint sweep) on a short time axis.
 FWI_CANDIDATES = ([dict(vec=2, rows=r, warps=w, tsteps=2) for r in (4, 8, 16) for w in (1, 2, 4)]
-                  + [dict(vec=2, rows=32, warps=w, tsteps=2) for w in (1, 2)])
+                  + [dict(vec=2, rows=32, warps=w, tsteps=2) for w in (1, 2)]
+                  # material ring with the task from the block index for the forward and recompute
+                  # launches (one warp per CTA, so the adjoint takes its uniform-task form too)
+                  + [dict(vec=2, rows=r, warps=1, tsteps=2, prefetch=4) for r in (8, 16, 32)])
 FWI_TUNE_STEPS = 160
 
 

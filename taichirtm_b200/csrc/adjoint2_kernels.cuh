@@ -50,12 +50,15 @@ struct AdjOut {
     float xx[VEC], zz[VEC], xz[VEC], u[VEC], w[VEC];
 };
 
-template <int VEC>
-__global__ void __launch_bounds__(256) adjoint2_kernel(const AdjParams p) {
+// UNI: launched with one warp per CTA, the task is blockIdx.x (the same
+// task as the general form computes then), so task-derived values are
+// provably warp-uniform; the arithmetic is unchanged.
+template <int VEC, bool UNI = false>
+__global__ void __launch_bounds__(UNI ? 32 : 256) adjoint2_kernel(const AdjParams p) {
     static_assert(VEC >= 2, "two steps per launch need two halo columns per side");
     constexpr int W = 30 * VEC;
     const int lane = threadIdx.x & 31;
-    const int task = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int task = UNI ? (int)blockIdx.x : (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (task >= p.n_work) return;
     const int4 wk = p.work[task];
     const ShotDev sh = p.shots[wk.x];

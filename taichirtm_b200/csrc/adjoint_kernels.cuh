@@ -127,11 +127,14 @@ __device__ __forceinline__ float adj_sponge(const float *prof, int fw, int nz, i
     return d >= 0 ? ldg_chk(prof + d) : 1.0f;
 }
 
-template <int VEC>
-__global__ void __launch_bounds__(256) adjoint_step_kernel(const AdjParams p) {
+// UNI: launched with one warp per CTA, the task is blockIdx.x (the same
+// task as the general form computes then), so task-derived values are
+// provably warp-uniform; the arithmetic is unchanged.
+template <int VEC, bool UNI = false>
+__global__ void __launch_bounds__(UNI ? 32 : 256) adjoint_step_kernel(const AdjParams p) {
     constexpr int W = 30 * VEC;
     const int lane = threadIdx.x & 31;
-    const int task = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int task = UNI ? (int)blockIdx.x : (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (task >= p.n_work) return;
     const int4 wk = p.work[task];
     const ShotDev sh = p.shots[wk.x];

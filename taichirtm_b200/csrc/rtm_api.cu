@@ -1388,8 +1388,13 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
                 if (p->tsteps == 2 && p->vec >= 2 && n - 1 >= start && n % GRAD_FOLD_STEPS != 0) {
                     float *fs2 = fwd_state(n - 1);
                     for (int f = 0; f < NADJ; ++f) ap.fwd2[f] = fld(fs2, f);
-                    if (p->vec == 2) adjoint2_kernel<2><<<blocks, 32 * warps, 0, s>>>(ap);
-                    else adjoint2_kernel<4><<<blocks, 32 * warps, 0, s>>>(ap);
+                    // one warp per CTA: the uniform-task instantiation (same task, same arithmetic)
+                    if (p->vec == 2) {
+                        if (warps == 1) adjoint2_kernel<2, true><<<blocks, 32, 0, s>>>(ap);
+                        else adjoint2_kernel<2><<<blocks, 32 * warps, 0, s>>>(ap);
+                    } else {
+                        adjoint2_kernel<4><<<blocks, 32 * warps, 0, s>>>(ap);
+                    }
                     CUDA_TRY(cudaGetLastError());
                     ++p->launches;
                     cur = 1 - cur;
@@ -1403,7 +1408,10 @@ int rtm_adjoint(rtm_plan *p, const float *wavelets, const float *resid, int ckpt
                 }
                 switch (p->vec) {
                     case 1: adjoint_step_kernel<1><<<blocks, 32 * warps, 0, s>>>(ap); break;
-                    case 2: adjoint_step_kernel<2><<<blocks, 32 * warps, 0, s>>>(ap); break;
+                    case 2:
+                        if (warps == 1) adjoint_step_kernel<2, true><<<blocks, 32, 0, s>>>(ap);
+                        else adjoint_step_kernel<2><<<blocks, 32 * warps, 0, s>>>(ap);
+                        break;
                     default: adjoint_step_kernel<4><<<blocks, 32 * warps, 0, s>>>(ap); break;
                 }
                 CUDA_TRY(cudaGetLastError());

@@ -339,7 +339,8 @@ def test_gradient_independent_of_launch_shape_and_autotuned():
     for tune in ("auto", dict(vec=2, rows=8, warps=2, tsteps=2), dict(vec=4, rows=5, warps=1),
                  dict(vec=1, rows=3, warps=4), dict(vec=2, rows=8, warps=2, tsteps=2, prefetch=3),
                  dict(vec=4, rows=6, warps=3, prefetch=3), dict(vec=4, rows=7, warps=2, tsteps=2),
-                 dict(vec=4, rows=6, warps=3, tsteps=2, prefetch=3)):
+                 dict(vec=4, rows=6, warps=3, tsteps=2, prefetch=3), dict(vec=2, rows=8, warps=1, tsteps=2),
+                 dict(vec=2, rows=5, warps=1, tsteps=2, prefetch=4), dict(vec=2, rows=7, warps=1)):
         from taichirtm_b200.fwi import FWIProblem
         from taichirtm_b200.plan import ShotGeometry
         prob = FWIProblem(P["nx"], P["nz"], P["dx"], P["dz"], P["fs"], P["nt"], P["fw"],
