@@ -18,6 +18,8 @@ CANDIDATES = [
     # prefetch 4 = the ring kernel with the task from the block index (one warp per CTA)
     dict(vec=2, rows=24, warps=1, tsteps=2, prefetch=4), dict(vec=2, rows=16, warps=1, tsteps=2, prefetch=4),
     dict(vec=2, rows=32, warps=1, tsteps=2, prefetch=4),
+    dict(vec=4, rows=16, warps=1, tsteps=2, prefetch=4), dict(vec=4, rows=24, warps=1, tsteps=2, prefetch=4),
+    dict(vec=4, rows=12, warps=1, tsteps=2, prefetch=4),
     dict(vec=2, rows=32, warps=1, tsteps=2, prefetch=3), dict(vec=2, rows=8, warps=2, tsteps=2, prefetch=3),
     dict(vec=2, rows=32, warps=1, tsteps=2), dict(vec=2, rows=16, warps=2, tsteps=2),
     dict(vec=2, rows=8, warps=2, tsteps=2), dict(vec=4, rows=32, warps=1, tsteps=2),
@@ -71,7 +73,7 @@ def _store(cache):
 def key(nz, shots, modes):
     name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
     rows = sum(s.nx for s in shots)
-    return f"{name}|nz={nz}|rows={rows}|shots={len(shots)}|modes={modes}|v8"
+    return f"{name}|nz={nz}|rows={rows}|shots={len(shots)}|modes={modes}|v9"
 
 
 def time_shape(make_plan, shots, tune, steps=TUNE_STEPS):

@@ -134,6 +134,21 @@ __global__ void __launch_bounds__(UNI ? 32 : 256) step2_kernel(const StepParams 
     const bool strip_far = __all_sync(FULL, nz - 1 - (c0 + VEC - 1) >= p.fw);
     auto all_in = [&](int i) { return strip_in && i >= 1 && i <= nx - 2; };
     auto all_far = [&](int i) { return strip_far && i >= p.fw && nx - 1 - i >= p.fw; };
+    // The general path's per-cell interior test and sponge coefficient,
+    // factored into a column part fixed for the task (here, once per lane)
+    // and a warp-uniform row part (ColRow below): the same cells are interior
+    // and the same sponge entry is chosen as by interior() and sponge_coef().
+    bool col_in[VEC], col_sp[VEC];
+    int col_db[VEC];
+    float col_cr[VEC];
+#pragma unroll
+    for (int q = 0; q < VEC; ++q) {
+        const int j = c0 + q;
+        col_in[q] = (unsigned)(j - 1) < (unsigned)(nz - 2);
+        col_db[q] = nz - 1 - j;  // distance to the bottom edge
+        col_sp[q] = col_db[q] >= 0 && col_db[q] < p.fw;
+        col_cr[q] = col_sp[q] ? ldg_chk(p.sponge + col_db[q]) : 1.0f;
+    }
     const long long soff = sh.state_off + (long long)(c0 + COL_OFF);
     const long long moff = (long long)sh.x0 * P + (long long)(c0 + COL_OFF);
     const float dt = p.dt, idx = p.inv_dx, idz = p.inv_dz;
@@ -241,10 +256,11 @@ __global__ void __launch_bounds__(UNI ? 32 : 256) step2_kernel(const StepParams 
     auto vel_cells = [&](auto fast_tag, int r, const Sig &sc, const Sig &sp, const Vel &vo, const Vel &ir,
                          Vel &out, float zz_nb, float xz_nb, float yz_nb) {
         constexpr bool FAST = decltype(fast_tag)::value;
+        const bool row_in = (unsigned)(r - 1) < (unsigned)(nx - 2);
 #pragma unroll
         for (int q = 0; q < VEC; ++q) {
             bool in = true;
-            if constexpr (!FAST) in = interior(r, c0 + q, nx, nz);
+            if constexpr (!FAST) in = row_in && col_in[q];
             if constexpr (PSV) {
                 float du, dw;
                 if constexpr (DIR == 0) {
@@ -363,14 +379,30 @@ __global__ void __launch_bounds__(UNI ? 32 : 256) step2_kernel(const StepParams 
     auto stress_cells = [&](auto fast_tag, int r, const Vel &va, const Vel &vb, const Sig &base, const Mat &m,
                             Sig &os, Vel &ov, float nu, float nw, float nv) {
         constexpr bool FAST = decltype(fast_tag)::value;
+        // row part of the sponge choice (sponge_coef): d = r if the row is in
+        // the left sponge and the cell is farther from the bottom, d = nx-1-r
+        // likewise for the right sponge, d = the bottom distance if that is
+        // in the sponge and no larger than both row distances (last wins)
+        bool row_in = true, ra = false, rb = false;
+        int dr = 0;
+        float cr_i = 1.0f, cr_dr = 1.0f;
+        if constexpr (!FAST) {
+            row_in = (unsigned)(r - 1) < (unsigned)(nx - 2);
+            dr = nx - 1 - r;
+            ra = r >= 0 && r < p.fw;
+            rb = dr >= 0 && dr < p.fw;
+            if (ra) cr_i = ldg_chk(p.sponge + r);
+            if (rb) cr_dr = ldg_chk(p.sponge + dr);
+        }
 #pragma unroll
         for (int q = 0; q < VEC; ++q) {
-            const int j = c0 + q;
             bool in = true;
             float cr = 1.0f;
             if constexpr (!FAST) {
-                in = interior(r, j, nx, nz);
-                cr = sponge_coef(p, nx, r, j);
+                in = row_in && col_in[q];
+                if (ra && col_db[q] > r) cr = cr_i;
+                if (rb && col_db[q] > dr) cr = cr_dr;
+                if (col_sp[q] && r >= col_db[q] && dr >= col_db[q]) cr = col_cr[q];
             }
             if constexpr (PSV) {
                 float u_x, u_z, w_x, w_z;
