@@ -5,6 +5,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -64,6 +65,32 @@ inline int append_row_table(int rows, int nz, int n, const int32_t *ij, int base
     }
     ptr.push_back((int)ent.size());
     return -1;
+}
+
+// Number of tasks at the end of a work list of n tasks that the tail split
+// cuts in two: 16 per SM (about one wave of the step kernels), at most a
+// quarter of the list.
+inline size_t tail_split_tasks(size_t n, int sms) { return std::min(n / 4, (size_t)(sms > 0 ? sms : 1) * 16); }
+
+// Replace the last `n` tasks {shot, strip word, ia, ib} of `work` that have
+// at least 2 rows by their two halves [ia, mid), [mid, ib), in order.
+inline void split_tail(std::vector<int4> &work, size_t n) {
+    n = std::min(n, work.size());
+    const size_t head = work.size() - n;
+    std::vector<int4> tail;
+    tail.reserve(2 * n);
+    for (size_t t = head; t < work.size(); ++t) {
+        const int4 w = work[t];
+        if (w.w - w.z >= 2) {
+            const int mid = w.z + (w.w - w.z + 1) / 2;
+            tail.push_back(make_int4(w.x, w.y, w.z, mid));
+            tail.push_back(make_int4(w.x, w.y, mid, w.w));
+        } else {
+            tail.push_back(w);
+        }
+    }
+    work.resize(head);
+    work.insert(work.end(), tail.begin(), tail.end());
 }
 
 }  // namespace rtm

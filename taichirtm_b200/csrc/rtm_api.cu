@@ -625,6 +625,18 @@ int rtm_plan_create(const rtm_grid *grid, int nshots, const rtm_shot *shots, con
         if (a.y != b.y) return a.y < b.y;
         return a.x < b.x;
     });
+    // Tail split: the last tasks of the list (the last blocks a launch
+    // dispatches) are cut into two halves of rows, so the final wave of a
+    // launch is made of short tasks and the SMs run out of work closer
+    // together.  Any partition of a shot's rows into tasks gives the same
+    // results; a half keeps its parent's no-source / no-receiver flags, which
+    // hold for any sub-range of rows.
+    {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            sms = 148;
+        split_tail(work, tail_split_tasks(work.size(), sms));
+    }
     p->n_work = (int)work.size();
     p->state_floats = (size_t)state_rows * p->pitch;
     const size_t mat_floats = (size_t)(g.nx + 2) * p->pitch;
