@@ -548,14 +548,17 @@ def main():
                     sample=f"shots 0..{nplain - 1} migrated one shot per plan (one shot per launch), "
                            "each plan with its own autotuned launch shape")
 
+    # the plain path, checkpointed RTM and gradient legs are one-GPU
+    # comparisons: run at N = 1 only, so an N-GPU run holds its GPUs for the
+    # sharded headline alone
     plain = None
-    if not args.no_plain and rank == 0:
+    if not args.no_plain and world == 1:
         plain = plain_rate(4)
 
     # checkpointed RTM: the same shots with sqrt(nt) checkpoints and the
     # forward wavefield recomputed segment by segment, batched vs plain
     ckpt_rtm = None
-    if not args.no_extra and rank == 0:
+    if not args.no_extra and world == 1:
         ck = dict(every=max(1, round(nt ** 0.5)), dtype=args.ckpt_dtype or "i16")
         rtm.migrate(wav, obs, isnap=ISNAP, checkpoint=ck)
         torch.cuda.synchronize()
@@ -578,7 +581,7 @@ def main():
                                  f"({ck['dtype']}) with recompute instead of snapshots")
 
     gradient = None
-    if not args.no_extra and rank == 0:
+    if not args.no_extra and world == 1:
         from taichirtm_b200 import benchmarks
         gradient = benchmarks.gradient_leg(nt=3000, steps=3, warmup=1, nplain=2)
 
