@@ -72,7 +72,7 @@ typedef struct {
 /* Kernel launch shape (autotuned by the Python layer; 0 = default). */
 typedef struct {
     int vec;        /* columns per lane: 1, 2 or 4 */
-    int rows;       /* rows per warp task */
+    int rows;       /* rows per warp task (the tasks a launch dispatches last get half as many) */
     int warps;      /* warps per CTA */
     int prefetch;   /* 1: software-pipelined row loads; 3: cp.async pipeline, rows 3 ahead in a
                        per-warp shared-memory ring (with tsteps 2: the material and 1/rho rows
