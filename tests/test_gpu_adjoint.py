@@ -2,6 +2,8 @@
 windowed shots.
 
 * dot-product test of the wavelet adjoint: <F w, g> = <w, F^T g>;
+* dot-product test in model space: <J dm, g> (FP64 centred differences of the
+  C restatement) = <dm, J^T g> (GPU adjoint) for a random cotangent g;
 * gradient w.r.t. (vp, vs, rho) against centred finite differences of the
   SAME discrete forward evaluated in FP64 by the C restatement, on 10 seeded
   random directions;
@@ -80,6 +82,45 @@ def _J_fp64(P, vp, vs, rho, obs):
                            dtype=np.float64, modes=1, check_interval=0)
     r = out["seis"][[0, 2]] - obs[[0, 2]]
     return 0.5 * float((r * r).sum())
+
+
+def test_dot_product_model_parameters_fp64():
+    """The adjoint as a linear operator in model space: for a random data-space
+    cotangent g (all three components) and seeded smooth model directions dm,
+    <J dm, g> with J dm the centred FP64 difference of the C restatement's
+    seismograms equals <dm, J^T g> from the GPU adjoint (through the autograd
+    path, w.r.t. vp, vs, rho), to 1e-4 relative."""
+    from taichirtm_b200.fwi import seismograms
+    P = _problem()
+    rng = np.random.default_rng(211)
+    prob = _fwi(P, ckpt=19)
+    m = [torch.tensor(x, dtype=torch.float64, device="cuda", requires_grad=True) for x in (P["vp"], P["vs"], P["rho"])]
+    d = seismograms(m[0], m[1], m[2], prob)
+    g = rng.standard_normal(tuple(d.shape))
+    g[1] = 0.0  # P-SV only: the SH component is not driven by (vp, vs, rho) through this problem's sources
+    d.backward(torch.as_tensor(g, dtype=d.dtype, device=d.device))
+    jtg = [x.grad.cpu().numpy() for x in m]
+    prob.close()
+
+    def seis64(vp, vs, rho):
+        lam, mu, rho_ = _lame(vp, vs, rho)
+        return c_oracle.forward(mu, lam, rho_, dx=P["dx"], dz=P["dz"], nt=P["nt"], fs=P["fs"], fw=P["fw"],
+                                src=P["src"], wu=P["wav"][0], wv=P["wav"][1], ww=P["wav"][2], rec=P["rec"],
+                                dtype=np.float64, modes=1, check_interval=0)["seis"]
+
+    errs = []
+    for _ in range(3):
+        dm = [_smooth(rng.standard_normal(P["vp"].shape), 2) for _ in range(3)]
+        dm = [s * x / np.abs(x).max() for s, x in zip((P["vp"].mean(), P["vs"].mean(), P["rho"].mean()), dm)]
+        eps = 1e-4
+        dp = seis64(*(v + eps * x for v, x in zip((P["vp"], P["vs"], P["rho"]), dm)))
+        dn = seis64(*(v - eps * x for v, x in zip((P["vp"], P["vs"], P["rho"]), dm)))
+        jdm = (dp - dn) / (2 * eps)
+        lhs = float((jdm[[0, 2]] * g[[0, 2]]).sum())
+        rhs = sum(float((a * b).sum()) for a, b in zip(jtg, dm))
+        errs.append(abs(lhs - rhs) / abs(lhs))
+    print(f"model-space dot product: relative errors {['%.2e' % e for e in errs]}")
+    assert max(errs) < 1e-4, errs
 
 
 def test_gradient_vs_centred_finite_differences_fp64():
