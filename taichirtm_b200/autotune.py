@@ -73,7 +73,7 @@ def _store(cache):
 def key(nz, shots, modes):
     name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
     rows = sum(s.nx for s in shots)
-    return f"{name}|nz={nz}|rows={rows}|shots={len(shots)}|modes={modes}|v9"
+    return f"{name}|nz={nz}|rows={rows}|shots={len(shots)}|modes={modes}|v10"
 
 
 def time_shape(make_plan, shots, tune, steps=TUNE_STEPS):
@@ -127,6 +127,8 @@ def best_shape(make_plan, nz, shots, modes, nt, candidates=None, refresh=False):
 # gradient itself (checkpointed forward + adjoint sweep) on a short time axis.
 FWI_CANDIDATES = ([dict(vec=2, rows=r, warps=w, tsteps=2) for r in (4, 8, 16) for w in (1, 2, 4)]
                   + [dict(vec=2, rows=32, warps=w, tsteps=2) for w in (1, 2)]
+                  # 24-row tasks: with the tail split, 1.7 % faster than 16 rows on the c4 gradient
+                  + [dict(vec=2, rows=24, warps=w, tsteps=2) for w in (2, 4)]
                   # material ring with the task from the block index for the forward and recompute
                   # launches (one warp per CTA, so the adjoint takes its uniform-task form too)
                   + [dict(vec=2, rows=r, warps=1, tsteps=2, prefetch=4) for r in (8, 16, 32)])
