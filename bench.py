@@ -494,22 +494,30 @@ def main():
         roofline["dram_frac"] = round(dram_gbs / peak, 4)
 
     # end to end through the public API: host inputs, device outputs read back
+    # into pinned host memory every step
     wav_h = wav.cpu().pin_memory()
     obs_h = obs.cpu().pin_memory()
+    host_img = torch.empty(tuple(stack.shape), dtype=stack.dtype).pin_memory()
     h2d = wav_h.numel() * 4 + obs_h.numel() * 4
-    d2h = stack.numel() * 8
+    d2h = host_img.numel() * 8
+
+    def e2e_step():
+        # observed data stay in pinned host memory: migrate copies them on a
+        # side stream while the forward pass runs (the backward reads them)
+        ff, fb, st = rtm.migrate(wav_h.to(dev, non_blocking=True), obs_h, isnap=ISNAP, check_interval=100)
+        if world > 1:
+            st = reduce_result(st, max(int(ff.max()), int(fb.max())))
+        host_img.copy_(st, non_blocking=True)
+        torch.cuda.current_stream().synchronize()  # the step's image is on the host
+
+    e2e_step()  # warm-up: the side stream's copy buffer is allocated here, not in the timed loop
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        # observed data stay in pinned host memory: migrate copies them on a
-        # side stream while the forward pass runs (the backward reads them)
-        ff, fb, st = rtm.migrate(wav_h.to(dev, non_blocking=True), obs_h, isnap=ISNAP, check_interval=100)
-        if world > 1:
-            st = reduce_result(st, max(int(ff.max()), int(fb.max())))
-        host_img = st.cpu()
+        e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
