@@ -3,6 +3,7 @@ FP32 restatement (same one-time FP64 set-up, Kahan imaging):
 
 * a shot without sources and a shot without receivers;
 * the smallest grid (3 x 3: one interior cell) and no sponge (FW = 0);
+* time axes of 1, 2, 3 and 7 steps (odd last steps with two steps per launch);
 * shot windows touching the first and the last model row, batched, with one
   and two steps per launch, equal to standalone runs on the cropped models.
 """
@@ -75,7 +76,8 @@ def test_shot_without_sources_or_receivers(case, tune):
 
 
 @pytest.mark.parametrize("tune", [dict(vec=1, rows=1, warps=1, prefetch=0), dict(vec=2, rows=2, warps=1, tsteps=2),
-                                  dict(vec=4, rows=8, warps=4, prefetch=3), dict(vec=2, rows=2, warps=3, tsteps=2, prefetch=3)])
+                                  dict(vec=4, rows=8, warps=4, prefetch=3), dict(vec=2, rows=2, warps=3, tsteps=2, prefetch=3),
+                                  dict(vec=4, rows=3, warps=1, tsteps=2, prefetch=4)])
 @pytest.mark.parametrize("grid", [(3, 3, 0), (5, 4, 0), (23, 17, 0), (23, 17, 4)])
 def test_smallest_grids_and_no_sponge(grid, tune):
     nx, nz, fw = grid
@@ -85,6 +87,30 @@ def test_smallest_grids_and_no_sponge(grid, tune):
     wav = np.zeros((3, 1, nt), np.float32)
     wav[:, 0] = _ricker(nt)[None] * np.array([[0.3], [0.6], [1.0]], np.float32)
     g, ref, bref = _gpu_vs_restatement(nx, nz, nt, fw, src, rec, wav, 3, tune)
+    assert g["flag"] == ref["flag"] == 0
+    assert np.array_equal(g["seis"], ref["seis"])
+    for c in range(3):
+        assert np.array_equal(g["snaps"][c], ref["snaps"][c])
+    assert np.array_equal(g["img"], bref["img"])
+    assert np.abs(g["seis"]).max() > 0
+
+
+@pytest.mark.parametrize("tune", [dict(vec=2, rows=4, warps=2, tsteps=1), dict(vec=2, rows=5, warps=1, tsteps=2, prefetch=4),
+                                  dict(vec=4, rows=3, warps=1, tsteps=2, prefetch=4)])
+@pytest.mark.parametrize("nt,isnap", [(1, 1), (2, 1), (3, 2), (7, 3)])
+def test_short_and_odd_time_axes(nt, isnap, tune):
+    """Time axes of 1, 2, 3 and 7 steps: an odd last step with two steps
+    per launch, no imaging step at all (nt 1), bit-exact against the FP32
+    restatement."""
+    nx, nz = 30, 24
+    src = np.array([[15, 5]], np.int32)
+    rec = np.array([[i, 2] for i in range(2, 28, 2)] + [[15, 5], [14, 5], [16, 5], [15, 4], [15, 6], [13, 7]],
+                   np.int32)  # a line, and cells at and around the source
+    wav = np.zeros((3, 1, nt), np.float32)
+    wav[:, 0, 0] = np.array([0.3, 0.6, 1.0], np.float32)
+    if nt > 1:
+        wav[:, 0, 1] = np.array([-0.1, 0.2, -0.5], np.float32)
+    g, ref, bref = _gpu_vs_restatement(nx, nz, nt, 4, src, rec, wav, isnap, tune)
     assert g["flag"] == ref["flag"] == 0
     assert np.array_equal(g["seis"], ref["seis"])
     for c in range(3):
